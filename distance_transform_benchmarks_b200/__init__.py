@@ -1,0 +1,221 @@
+"""B200-native generalised geodesic distance transform (GGDT).
+
+Python mirror of the reference library's entry points (namespace ``dt``,
+dt/include/dt/generalised_distance_transform.hpp:7-27 and dt/include/dt/transfert.hpp:9-17) over the C ABI
+of include/dtb.h.  Torch tensors serve as containers (device memory, streams); every distance is computed by
+the CUDA kernels in libdtb.so -- there is no fallback path.
+
+Images are ``uint8`` tensors of shape ``[H, W]`` (gray) or ``[H, W, 3]`` (rgb8), seed masks ``uint8 [H, W]``
+(non-zero = seed), distances ``float32 [H, W]``.  Rows may be padded (``stride(0)`` is the pitch).  Inputs on the
+CPU are staged to the device by the library, as the reference's ``host_to_device`` does for its callers.
+"""
+import ctypes
+import threading
+
+import numpy as np
+import torch
+
+from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_GPU, DtbError, DtbImage,
+                      DtbStats, lib)
+
+__all__ = [
+    "Context", "DtbError", "default_context", "generalised_distance_transform",
+    "generalised_distance_transform_blocks", "generalised_distance_transform_task", "geodesic_distance_transform",
+    "geodesic_distance_transform_batch", "host_to_device", "device_to_host", "image_view", "DEFAULT_V",
+]
+
+DEFAULT_V = 1e10  # reference default, generalised_distance_transform.hpp:8
+
+
+class Context:
+    """A dtb_context: owns the device scratch of the calls made through it."""
+
+    def __init__(self, device=None):
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = int(device)
+        self._h = ctypes.c_void_p()
+        st = lib().dtb_context_create(self.device, ctypes.byref(self._h))
+        if st != 0:
+            raise DtbError(st, "dtb_context_create(%d) failed (an sm_100 device is required)" % self.device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, status):
+        if status != 0:
+            raise DtbError(status, lib().dtb_context_message(self._h).decode())
+
+    def stats(self):
+        s = DtbStats()
+        self.check(lib().dtb_last_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in DtbStats._fields_}
+
+    def sync(self, stream=None):
+        self.check(lib().dtb_sync(self._h, ctypes.c_void_p(_stream_ptr(stream))))
+
+    def close(self):
+        if self._h:
+            lib().dtb_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_ctx_lock = threading.Lock()
+_contexts = {}
+
+
+def default_context(device=None):
+    if device is None:
+        device = torch.cuda.current_device()
+    with _ctx_lock:
+        c = _contexts.get(device)
+        if c is None:
+            c = _contexts[device] = Context(device)
+        return c
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def image_view(t, elem_size=None):
+    """dtb_image view of a tensor ([H, W] or [H, W, C], rows contiguous)."""
+    if isinstance(t, np.ndarray):
+        t = torch.from_numpy(t)
+    if t.dim() == 3:
+        h, w, c = t.shape
+        if t.stride(2) != 1 or t.stride(1) != c:
+            raise ValueError("pixels of a [H, W, C] image must be contiguous")
+    elif t.dim() == 2:
+        h, w = t.shape
+        c = 1
+        if t.stride(1) != 1 and w > 1:
+            raise ValueError("rows must be contiguous")
+    else:
+        raise ValueError("expected a [H, W] or [H, W, C] tensor")
+    es = t.element_size() * c
+    if elem_size is not None and es != elem_size:
+        raise ValueError("element size %d, expected %d" % (es, elem_size))
+    pitch = t.stride(0) * t.element_size() if h > 1 else w * es
+    kind = DTB_GPU if t.is_cuda else DTB_CPU
+    return DtbImage(t.data_ptr() if t.numel() else None, w, h, pitch, es, kind)
+
+
+def _as_tensor(x):
+    if isinstance(x, np.ndarray):
+        return torch.from_numpy(np.ascontiguousarray(x))
+    return x
+
+
+def _dist_like(img, dist):
+    if dist is not None:
+        return dist
+    h, w = img.shape[0], img.shape[1]
+    return torch.empty((h, w), dtype=torch.float32, device=img.device)
+
+
+def _ctx_for(t, ctx):
+    if ctx is not None:
+        return ctx
+    dev = t.device.index if t.is_cuda else None
+    return default_context(dev)
+
+
+def _ref_call(img, mask, lam, v, dist, rounds, ctx, stream, fma):
+    img, mask = _as_tensor(img), _as_tensor(mask)
+    dist = _dist_like(img, dist)
+    ctx = _ctx_for(img, ctx)
+    if stream is None and img.is_cuda:
+        stream = torch.cuda.current_stream(img.device)
+    vi, vm, vd = image_view(img, 1), image_view(mask, 1), image_view(dist, 4)
+    flags = (DTB_FLAG_ROUNDS if rounds else 0) | (0 if fma else DTB_FLAG_REF_NO_FMA)
+    ctx.check(lib().dtb_gdt_ref(ctx.handle, ctypes.byref(vi), ctypes.byref(vm), ctypes.byref(vd), float(lam), float(v),
+                                flags, ctypes.c_void_p(_stream_ptr(stream))))
+    return dist
+
+
+def generalised_distance_transform(img, mask, lam, v=DEFAULT_V, dist=None, *, ctx=None, stream=None, fma=True):
+    """Reference weight (C8, lambda blend): dt::generalised_distance_transform
+    (reference dt/src/generalised_distance_transform.cu:101-148).  Returns ``dist`` (allocated if None)."""
+    return _ref_call(img, mask, lam, v, dist, False, ctx, stream, fma)
+
+
+def generalised_distance_transform_blocks(img, mask, lam, v=DEFAULT_V, dist=None, *, ctx=None, stream=None, fma=True):
+    """dt::generalised_distance_transform_blocks (reference _blocks.cu:114-184): host-driven rounds over active
+    tiles.  Same result as the other two variants."""
+    return _ref_call(img, mask, lam, v, dist, True, ctx, stream, fma)
+
+
+def generalised_distance_transform_task(img, mask, lam, v=DEFAULT_V, dist=None, *, ctx=None, stream=None, fma=True):
+    """dt::generalised_distance_transform_task (reference _task.cu:152-207): persistent tile queue."""
+    return _ref_call(img, mask, lam, v, dist, False, ctx, stream, fma)
+
+
+def geodesic_distance_transform(img, mask, gamma, v=DEFAULT_V, dist=None, *, rounds=False, ctx=None, stream=None):
+    """C4 geodesic distance with w = sqrt(1 + gamma^2 |dI|^2), gray or rgb8 (dtb_gdt)."""
+    img, mask = _as_tensor(img), _as_tensor(mask)
+    dist = _dist_like(img, dist)
+    ctx = _ctx_for(img, ctx)
+    if stream is None and img.is_cuda:
+        stream = torch.cuda.current_stream(img.device)
+    es = 3 if img.dim() == 3 else 1
+    vi, vm, vd = image_view(img, es), image_view(mask, 1), image_view(dist, 4)
+    ctx.check(lib().dtb_gdt(ctx.handle, ctypes.byref(vi), ctypes.byref(vm), ctypes.byref(vd), float(gamma), float(v),
+                            DTB_FLAG_ROUNDS if rounds else 0, ctypes.c_void_p(_stream_ptr(stream))))
+    return dist
+
+
+def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=None, *, rounds=False, ctx=None,
+                                      stream=None, asynchronous=False):
+    """Ragged batch in one persistent launch over a shared tile queue (dtb_gdt_batch)."""
+    n = len(imgs)
+    imgs = [_as_tensor(t) for t in imgs]
+    masks = [_as_tensor(t) for t in masks]
+    if dists is None:
+        dists = [_dist_like(t, None) for t in imgs]
+    if n == 0:
+        return dists
+    ctx = _ctx_for(imgs[0], ctx)
+    if stream is None and imgs[0].is_cuda:
+        stream = torch.cuda.current_stream(imgs[0].device)
+    vi = (DtbImage * n)(*[image_view(t, 3 if t.dim() == 3 else 1) for t in imgs])
+    vm = (DtbImage * n)(*[image_view(t, 1) for t in masks])
+    vd = (DtbImage * n)(*[image_view(t, 4) for t in dists])
+    g = (ctypes.c_float * n)(*[float(x) for x in gammas])
+    flags = (DTB_FLAG_ROUNDS if rounds else 0) | (DTB_FLAG_ASYNC if asynchronous else 0)
+    ctx.check(lib().dtb_gdt_batch(ctx.handle, n, vi, vm, vd, g, float(v), flags, ctypes.c_void_p(_stream_ptr(stream))))
+    return dists
+
+
+def host_to_device(t, stream=None):
+    """dt::host_to_device (reference dt/src/transfert.cpp:10-18): pitched copy into new device memory."""
+    t = _as_tensor(t)
+    out = torch.empty_like(t, device="cuda")
+    es = t.element_size() * (t.shape[2] if t.dim() == 3 else 1)
+    st = lib().dtb_host_to_device(ctypes.byref(image_view(t, es)), ctypes.byref(image_view(out, es)),
+                                  ctypes.c_void_p(_stream_ptr(stream)))
+    if st != 0:
+        raise DtbError(st, "Unable to transfert host to device")
+    return out
+
+
+def device_to_host(t, stream=None):
+    """dt::device_to_host (reference dt/src/transfert.cpp:20-28)."""
+    out = torch.empty_like(t, device="cpu")
+    es = t.element_size() * (t.shape[2] if t.dim() == 3 else 1)
+    st = lib().dtb_device_to_host(ctypes.byref(image_view(t, es)), ctypes.byref(image_view(out, es)),
+                                  ctypes.c_void_p(_stream_ptr(stream)))
+    if st != 0:
+        raise DtbError(st, "Unable to transfert device to host")
+    return out

@@ -1,0 +1,121 @@
+"""ctypes declarations of the native libraries (include/dtb.h and the generator library).
+
+Loading fails loudly: there is no Python or CPU fallback for the distance transform.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDTB_PATH = os.path.join(HERE, "libdtb.so")
+LIBHOST_PATH = os.path.join(HERE, "libdtb_host.so")
+
+DTB_CPU = 0
+DTB_GPU = 1
+
+DTB_FLAG_ASYNC = 0x1
+DTB_FLAG_ROUNDS = 0x2
+DTB_FLAG_REF_NO_FMA = 0x4
+
+STATUS_NAMES = {
+    0: "DTB_OK", 1: "DTB_ERR_INVALID_ARG", 2: "DTB_ERR_CUDA", 3: "DTB_ERR_OUT_OF_MEMORY", 4: "DTB_ERR_TIMEOUT",
+    5: "DTB_ERR_DEVICE", 6: "DTB_ERR_NO_DEVICE", 7: "DTB_ERR_CAPACITY",
+}
+
+# Every symbol include/dtb.h declares (checked by the CPU test suite).
+DTB_SYMBOLS = [
+    "dtb_abi_version", "dtb_status_string", "dtb_context_create", "dtb_context_destroy", "dtb_context_message",
+    "dtb_last_stats", "dtb_sync", "dtb_gdt_ref", "dtb_gdt", "dtb_gdt_batch", "dtb_host_to_device",
+    "dtb_device_to_host",
+]
+
+
+class DtbImage(ctypes.Structure):
+    """dtb_image: the fields of dt::image2d_view<void> (reference dt/include/dt/image2d_view.hpp:117-123)."""
+    _fields_ = [
+        ("buffer", ctypes.c_void_p),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("pitch", ctypes.c_int32),
+        ("elem_size", ctypes.c_int32),
+        ("memory_kind", ctypes.c_int32),
+    ]
+
+
+class DtbStats(ctypes.Structure):
+    _fields_ = [
+        ("tiles", ctypes.c_uint64),
+        ("tile_visits", ctypes.c_uint64),
+        ("phases", ctypes.c_uint64),
+        ("activations", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint64),
+        ("device_error", ctypes.c_uint32),
+        ("device_error_info", ctypes.c_uint32),
+    ]
+
+
+class DtbError(RuntimeError):
+    """A dtb_* call returned a non-zero status (the reference throws std::runtime_error in these cases)."""
+
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__("%s: %s" % (STATUS_NAMES.get(status, status), message))
+
+
+_lib = None
+_host = None
+
+
+def lib():
+    """The CUDA library; raises if it was not built (run __graft_entry__.build())."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBDTB_PATH):
+            raise RuntimeError("libdtb.so is missing at %s: build it with __graft_entry__.build()" % LIBDTB_PATH)
+        L = ctypes.CDLL(LIBDTB_PATH)
+        P, I32, U32, F = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32, ctypes.c_float
+        IMG = ctypes.POINTER(DtbImage)
+        L.dtb_abi_version.restype = I32
+        L.dtb_status_string.restype = ctypes.c_char_p
+        L.dtb_status_string.argtypes = [I32]
+        L.dtb_context_create.restype = I32
+        L.dtb_context_create.argtypes = [I32, ctypes.POINTER(P)]
+        L.dtb_context_destroy.restype = None
+        L.dtb_context_destroy.argtypes = [P]
+        L.dtb_context_message.restype = ctypes.c_char_p
+        L.dtb_context_message.argtypes = [P]
+        L.dtb_last_stats.restype = I32
+        L.dtb_last_stats.argtypes = [P, ctypes.POINTER(DtbStats)]
+        L.dtb_sync.restype = I32
+        L.dtb_sync.argtypes = [P, P]
+        L.dtb_gdt_ref.restype = I32
+        L.dtb_gdt_ref.argtypes = [P, IMG, IMG, IMG, F, F, U32, P]
+        L.dtb_gdt.restype = I32
+        L.dtb_gdt.argtypes = [P, IMG, IMG, IMG, F, F, U32, P]
+        L.dtb_gdt_batch.restype = I32
+        L.dtb_gdt_batch.argtypes = [P, I32, IMG, IMG, IMG, ctypes.POINTER(F), F, U32, P]
+        L.dtb_host_to_device.restype = I32
+        L.dtb_host_to_device.argtypes = [IMG, IMG, P]
+        L.dtb_device_to_host.restype = I32
+        L.dtb_device_to_host.argtypes = [IMG, IMG, P]
+        _lib = L
+    return _lib
+
+
+def host():
+    """The host-only generator library."""
+    global _host
+    if _host is None:
+        if not os.path.exists(LIBHOST_PATH):
+            raise RuntimeError("libdtb_host.so is missing at %s: build it with __graft_entry__.build()" % LIBHOST_PATH)
+        H = ctypes.CDLL(LIBHOST_PATH)
+        P, I, I64, U64, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+        H.dtbg_blobs_gray.restype = None
+        H.dtbg_blobs_gray.argtypes = [U64, I, I, I, D, D, D, D, D, P, I64]
+        H.dtbg_voronoi_rgb.restype = None
+        H.dtbg_voronoi_rgb.argtypes = [U64, I, I, I, D, P, I64]
+        H.dtbg_maze_gray.restype = I
+        H.dtbg_maze_gray.argtypes = [U64, I, I, I, I, I, P, I64, ctypes.POINTER(I), ctypes.POINTER(I)]
+        H.dtbg_draw_disks.restype = None
+        H.dtbg_draw_disks.argtypes = [P, I64, I, I, I, P, P, P]
+        _host = H
+    return _host

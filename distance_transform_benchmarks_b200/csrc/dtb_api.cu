@@ -1,0 +1,694 @@
+// dtb_api.cu -- kernels and the C ABI (include/dtb.h) of the B200 GGDT.
+//
+// Host flow of one call (all stream-ordered, no host round trip except in the plain rounds path):
+//   descriptor tables + TMA tensor maps -> device (one copy), queue header reset,
+//   ggdt_scan (seed tiles), ggdt_persistent (cooperative, all tiles of all images), ggdt_finalize.
+// The reference's host drivers (dt/src/generalised_distance_transform*.cu) instead poll a managed flag
+// after every round; the plain path (DTB_FLAG_ROUNDS) keeps that structure as the per-image baseline.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dtb.h"
+#include "dtb_kernels.cuh"
+#include "dtb_internal.h"
+
+using namespace dtb;
+
+// ======================================================================================================
+// Kernels
+// ======================================================================================================
+namespace dtb {
+
+// Seed-tile scan: one warp per tile, every mask byte read once (lane = row, two 16-byte loads per row).
+// Writes the tile state (image index, SEED, PENDING / VISITED) and queues (or marks active) seed tiles.
+__global__ void __launch_bounds__(128) ggdt_scan(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
+                                                 int n, uint32_t total, uint32_t* __restrict__ states, Queue q,
+                                                 uint8_t* __restrict__ active, int warm) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = warp; t < total; t += nwarps) {
+    const uint32_t img = image_of_tile(tile_base, n, t);
+    const ImgDesc& dd = descs[img];
+    const uint32_t local = t - dd.tile_base;
+    const int tx = (int)(local % (uint32_t)dd.tiles_x), ty = (int)(local / (uint32_t)dd.tiles_x);
+    const int x0 = tx * TILE, y0 = ty * TILE;
+    const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
+    bool nz = false;
+    if (lane < vh) {
+      const uint8_t* row = dd.mask + (int64_t)(y0 + lane) * dd.mask_pitch + x0;
+      if (vw == TILE && (reinterpret_cast<uintptr_t>(row) & 15u) == 0) {
+        const uint4 a = reinterpret_cast<const uint4*>(row)[0];
+        const uint4 b = reinterpret_cast<const uint4*>(row)[1];
+        nz = (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
+      } else {
+        for (int c = 0; c < vw; ++c) nz |= row[c] != 0;
+      }
+    }
+    nz = __any_sync(~0u, nz);
+    if (lane == 0) {
+      uint32_t st = (img << ST_IMG_SHIFT) | (warm ? ST_VISITED : 0u);
+      if (nz) st |= ST_SEED | (active ? 0u : ST_PENDING);
+      states[t] = st;
+      if (nz) {
+        if (active) active[t] = 1;
+        else queue_push(q, t);
+      }
+    }
+  }
+}
+
+// Persistent tile worker.  Every warp loops: pop a tile, visit it, until the queue drains.
+template <int MODE, int WPC, int MINB>
+__global__ void __launch_bounds__(WPC * 32, MINB)
+    ggdt_persistent(const ImgDesc* __restrict__ descs, const CUtensorMap* __restrict__ tmaps, uint32_t* states, Queue q) {
+  extern __shared__ uint8_t smem_raw[];
+  WarpSmem& sm = warp_slot(smem_raw);
+  warp_slot_init(sm);
+  uint32_t parity = 0;
+  const QueueSched sch{q, states};
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    uint32_t t = POP_NONE, old = 0;
+    if (lane == 0) {
+      t = queue_pop(q);
+      if (t != POP_NONE) old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
+    }
+    t = __shfl_sync(~0u, t, 0);
+    if (t == POP_NONE) break;
+    old = __shfl_sync(~0u, old, 0);
+    const uint32_t img = old >> ST_IMG_SHIFT;
+    const ImgDesc dd = descs[img];
+    visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch);
+  }
+}
+
+// One host-driven round: one warp per tile, inactive tiles return at once.
+template <int MODE, int WPC>
+__global__ void __launch_bounds__(WPC * 32)
+    ggdt_round(const ImgDesc* __restrict__ descs, const CUtensorMap* __restrict__ tmaps, uint32_t* states,
+               const uint8_t* __restrict__ active, uint8_t* next_active, uint32_t* changed, uint32_t total, Queue q) {
+  extern __shared__ uint8_t smem_raw[];
+  WarpSmem& sm = warp_slot(smem_raw);
+  const uint32_t t = blockIdx.x * WPC + (threadIdx.x >> 5);
+  if (t >= total || !active[t]) return;
+  warp_slot_init(sm);
+  uint32_t parity = 0;
+  const uint32_t old = ld_volatile(&states[t]);
+  const uint32_t img = old >> ST_IMG_SHIFT;
+  const RoundSched sch{q, states, next_active, changed};
+  const ImgDesc dd = descs[img];
+  visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch);
+}
+
+// Tiles never reached keep uninitialised memory: write v there.
+__global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
+                                                     int n, uint32_t total, const uint32_t* __restrict__ states) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t t = warp; t < total; t += nwarps) {
+    if (states[t] & ST_VISITED) continue;
+    const uint32_t img = image_of_tile(tile_base, n, t);
+    const ImgDesc& dd = descs[img];
+    const uint32_t local = t - dd.tile_base;
+    const int tx = (int)(local % (uint32_t)dd.tiles_x), ty = (int)(local / (uint32_t)dd.tiles_x);
+    const int x0 = tx * TILE, y0 = ty * TILE;
+    const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
+    if (lane < vw)
+      for (int y = 0; y < vh; ++y) dist_row(dd, y0 + y)[x0 + lane] = dd.v;
+  }
+}
+
+}  // namespace dtb
+
+// ======================================================================================================
+// Host side
+// ======================================================================================================
+namespace {
+
+constexpr int PERSIST_WPC = 4;
+constexpr int PERSIST_MINB = 4;
+constexpr int ROUND_WPC = 4;
+constexpr size_t SMEM_SLOT = sizeof(WarpSmem);
+constexpr size_t PERSIST_SMEM = PERSIST_WPC * SMEM_SLOT + 128;
+constexpr size_t ROUND_SMEM = ROUND_WPC * SMEM_SLOT + 128;
+constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+uint32_t next_pow2(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+struct dtb_context_s {
+  int device = 0;
+  int num_sms = 0;
+  int persist_blocks_per_sm[2] = {0, 0};  // per weight mode
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  void* dscratch = nullptr;
+  size_t dscratch_size = 0;
+  void* dstage = nullptr;
+  size_t dstage_size = 0;
+  std::vector<uint8_t> hstage;
+  std::string msg;
+  dtb_stats stats{};
+  // Asynchronous bookkeeping: header of the last enqueued run and the stream it ran on.
+  QueueHdr* last_hdr = nullptr;
+  uint64_t last_tiles = 0;
+  cudaStream_t last_stream = nullptr;
+  bool async_pending = false;
+  std::mutex mu;
+};
+
+namespace {
+
+dtb_status fail(dtb_context ctx, dtb_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->msg = buf;
+  return s;
+}
+
+dtb_status cuda_fail(dtb_context ctx, cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+  return fail(ctx, DTB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define DTB_CUDA(ctx, call)                                         \
+  do {                                                              \
+    cudaError_t e_ = (call);                                        \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);      \
+  } while (0)
+
+dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
+  if (*size >= need) return DTB_OK;
+  if (*p) {
+    cudaDeviceSynchronize();
+    cudaFree(*p);
+    *p = nullptr;
+    *size = 0;
+  }
+  const size_t sz = align_up(need + need / 4, 1 << 20);
+  cudaError_t e = cudaMalloc(p, sz);
+  if (e != cudaSuccess) { *p = nullptr; return cuda_fail(ctx, e, "cudaMalloc(scratch)"); }
+  *size = sz;
+  return DTB_OK;
+}
+
+bool encode_u8_2d(dtb_context ctx, CUtensorMap* out, const void* base, uint64_t row_bytes, uint64_t rows, uint64_t pitch,
+                  uint32_t box_w, uint32_t box_h) {
+  cuuint64_t dims[2] = {row_bytes, rows};
+  cuuint64_t strides[1] = {pitch};
+  cuuint32_t box[2] = {box_w, box_h};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = ctx->encode(out, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------------
+// Jobs: one image each, already resolved to device memory with the alignment TMA needs.
+// ------------------------------------------------------------------------------------------------------
+namespace dtb {
+
+dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name, int elem_a, int elem_b) {
+  if (!im) return fail(ctx, DTB_ERR_INVALID_ARG, "%s is NULL", name);
+  if (im->width < 0 || im->height < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "%s has a negative size", name);
+  if (im->elem_size != elem_a && im->elem_size != elem_b)
+    return fail(ctx, DTB_ERR_INVALID_ARG, "%s: unsupported elem_size %d", name, im->elem_size);
+  if (im->memory_kind != DTB_CPU && im->memory_kind != DTB_GPU)
+    return fail(ctx, DTB_ERR_INVALID_ARG, "%s: unknown memory_kind %d", name, im->memory_kind);
+  if (im->width > 0 && im->height > 0) {
+    if (!im->buffer) return fail(ctx, DTB_ERR_INVALID_ARG, "%s: NULL buffer", name);
+    if ((int64_t)im->pitch < (int64_t)im->width * im->elem_size)
+      return fail(ctx, DTB_ERR_INVALID_ARG, "%s: pitch %d < width * elem_size", name, im->pitch);
+  }
+  return DTB_OK;
+}
+
+// Resolves the user views of one or more images into device jobs, staging copies where the user memory is
+// on the host or lacks the 16-byte alignment of TMA (input) / 4-byte alignment of float rows (output).
+struct Staged {
+  const dtb_image* user;
+  uint8_t* dev;
+  int64_t pitch;
+  bool copy_in;
+  bool copy_out;
+};
+
+static bool tma_ok(const dtb_image* im) {
+  return im->memory_kind == DTB_GPU && (reinterpret_cast<uintptr_t>(im->buffer) & 15u) == 0 && (im->pitch & 15) == 0;
+}
+static bool dist_ok(const dtb_image* im) {
+  return im->memory_kind == DTB_GPU && (reinterpret_cast<uintptr_t>(im->buffer) & 3u) == 0 && (im->pitch & 3) == 0;
+}
+
+dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_image* const* imgs,
+                    const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream) {
+  const int n = (int)jobs_in.size();
+  std::vector<Job> jobs = jobs_in;
+
+  // Serialise with a previous asynchronous call on another stream (the scratch is shared).
+  if (ctx->async_pending && ctx->last_stream != stream) {
+    DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
+  }
+
+  // ---- staging of inputs / outputs that are on the host or not aligned for TMA ----
+  std::vector<Staged> staged;
+  size_t stage_bytes = 0;
+  for (int i = 0; i < n; ++i) {
+    if (jobs[i].width == 0 || jobs[i].height == 0) continue;
+    const dtb_image* in3[3] = {imgs[i], masks[i], dists[i]};
+    for (int k = 0; k < 3; ++k) {
+      const dtb_image* u = in3[k];
+      const bool ok = (k < 2) ? tma_ok(u) : dist_ok(u);
+      if (ok) continue;
+      const int64_t row = (int64_t)u->width * u->elem_size;
+      const int64_t pitch = (int64_t)align_up((size_t)row, 128);
+      staged.push_back({u, reinterpret_cast<uint8_t*>(stage_bytes), pitch, k < 2, k == 2});
+      stage_bytes += align_up((size_t)(pitch * u->height), 256);
+    }
+  }
+  if (stage_bytes) {
+    dtb_status s = grow(ctx, &ctx->dstage, &ctx->dstage_size, stage_bytes);
+    if (s != DTB_OK) return s;
+    for (auto& st : staged) st.dev = reinterpret_cast<uint8_t*>(ctx->dstage) + reinterpret_cast<uintptr_t>(st.dev);
+  }
+  auto find_stage = [&](const dtb_image* u) -> const Staged* {
+    for (auto& st : staged)
+      if (st.user == u) return &st;
+    return nullptr;
+  };
+  for (int i = 0; i < n; ++i) {
+    if (jobs[i].width == 0 || jobs[i].height == 0) continue;
+    if (const Staged* st = find_stage(imgs[i])) { jobs[i].img = st->dev; jobs[i].img_pitch = st->pitch; }
+    if (const Staged* st = find_stage(masks[i])) { jobs[i].mask = st->dev; jobs[i].mask_pitch = st->pitch; }
+    if (const Staged* st = find_stage(dists[i])) { jobs[i].dist = reinterpret_cast<float*>(st->dev); jobs[i].dist_pitch = st->pitch; }
+  }
+  for (auto& st : staged) {
+    if (!st.copy_in) continue;
+    const dtb_image* u = st.user;
+    const cudaMemcpyKind kind = u->memory_kind == DTB_CPU ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    DTB_CUDA(ctx, cudaMemcpy2DAsync(st.dev, (size_t)st.pitch, u->buffer, (size_t)u->pitch, (size_t)u->width * u->elem_size,
+                                    (size_t)u->height, kind, stream));
+  }
+
+  // ---- descriptor tables ----
+  uint64_t total64 = 0;
+  std::vector<uint32_t> base(n + 1);
+  for (int i = 0; i < n; ++i) {
+    base[i] = (uint32_t)total64;
+    total64 += (uint64_t)jobs[i].tiles_x() * jobs[i].tiles_y();
+  }
+  base[n] = (uint32_t)total64;
+  if (total64 >= (1ull << 31) || n >= (1 << 23)) return fail(ctx, DTB_ERR_CAPACITY, "too many tiles (%llu) or images", (unsigned long long)total64);
+  const uint32_t total = (uint32_t)total64;
+  const bool rounds = (flags & DTB_FLAG_ROUNDS) != 0;
+  const int mode = n > 0 ? jobs[0].mode : MODE_NS;
+  for (int i = 1; i < n; ++i)
+    if (jobs[i].mode != mode) return fail(ctx, DTB_ERR_INVALID_ARG, "one call covers images of one weight mode");
+
+  const uint32_t workers = (uint32_t)(ctx->num_sms * ctx->persist_blocks_per_sm[mode] * PERSIST_WPC);
+  const uint32_t cap = next_pow2(2u * (total + workers + 64u));
+
+  size_t off = 0;
+  const size_t o_hdr = off;   off = align_up(off + sizeof(QueueHdr), 256);
+  const size_t o_states = off; off = align_up(off + 4ull * std::max<uint32_t>(total, 1), 256);
+  const size_t o_ring = off;  off = align_up(off + 4ull * cap, 256);
+  const size_t o_desc = off;  off = align_up(off + sizeof(ImgDesc) * (size_t)std::max(n, 1), 256);
+  const size_t o_tmap = off;  off = align_up(off + sizeof(CUtensorMap) * 2 * (size_t)std::max(n, 1), 256);
+  const size_t o_base = off;  off = align_up(off + 4ull * (n + 1), 256);
+  const size_t o_act = off;   off = align_up(off + (rounds ? 2ull * std::max<uint32_t>(total, 1) : 0), 256);
+  const size_t o_chg = off;   off = align_up(off + 4, 256);
+  dtb_status s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, off);
+  if (s != DTB_OK) return s;
+  uint8_t* dbase = reinterpret_cast<uint8_t*>(ctx->dscratch);
+
+  // Host image of [desc | tmaps | tile_base].
+  const size_t tbl_bytes = o_act - o_desc;
+  ctx->hstage.assign(tbl_bytes, 0);
+  ImgDesc* hdesc = reinterpret_cast<ImgDesc*>(ctx->hstage.data());
+  CUtensorMap* htm = reinterpret_cast<CUtensorMap*>(ctx->hstage.data() + (o_tmap - o_desc));
+  uint32_t* hbase = reinterpret_cast<uint32_t*>(ctx->hstage.data() + (o_base - o_desc));
+  for (int i = 0; i < n; ++i) {
+    const Job& j = jobs[i];
+    ImgDesc& d = hdesc[i];
+    d.img = j.img; d.mask = j.mask; d.dist = j.dist;
+    d.img_pitch = j.img_pitch; d.mask_pitch = j.mask_pitch; d.dist_pitch = j.dist_pitch;
+    d.width = j.width; d.height = j.height; d.channels = j.channels;
+    d.tiles_x = j.tiles_x(); d.tiles_y = j.tiles_y();
+    d.tile_base = base[i];
+    d.g2 = j.g2; d.v = j.v; d.l_eucl = j.l_eucl; d.l_grad = j.l_grad;
+    d.mode = j.mode; d.ref_fma = j.ref_fma;
+    hbase[i] = base[i];
+    if (j.width > 0 && j.height > 0) {
+      const uint32_t bw = j.channels == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY;
+      if (!encode_u8_2d(ctx, &htm[2 * i], j.img, (uint64_t)j.width * j.channels, (uint64_t)j.height, (uint64_t)j.img_pitch, bw,
+                        IMG_BOX_ROWS))
+        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the image layout", i);
+      if (!encode_u8_2d(ctx, &htm[2 * i + 1], j.mask, (uint64_t)j.width, (uint64_t)j.height, (uint64_t)j.mask_pitch, TILE, TILE))
+        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the mask layout", i);
+    }
+  }
+  hbase[n] = base[n];
+
+  QueueHdr* hdr = reinterpret_cast<QueueHdr*>(dbase + o_hdr);
+  uint32_t* states = reinterpret_cast<uint32_t*>(dbase + o_states);
+  uint32_t* ring = reinterpret_cast<uint32_t*>(dbase + o_ring);
+  const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + o_desc);
+  const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + o_tmap);
+  const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + o_base);
+  uint8_t* act0 = dbase + o_act;
+  uint8_t* act1 = dbase + o_act + total;
+  uint32_t* changed = reinterpret_cast<uint32_t*>(dbase + o_chg);
+
+  DTB_CUDA(ctx, cudaMemcpyAsync(dbase + o_desc, ctx->hstage.data(), tbl_bytes, cudaMemcpyHostToDevice, stream));
+  DTB_CUDA(ctx, cudaMemsetAsync(hdr, 0, sizeof(QueueHdr), stream));
+  DTB_CUDA(ctx, cudaMemsetAsync(ring, 0, 4ull * cap, stream));
+
+  // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
+  // this cap, which only turns a scheduling bug into an error instead of an endless run.
+  const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * total + (1ull << 20));
+  Queue q{hdr, ring, cap - 1, DEFAULT_TIMEOUT_NS, (uint32_t)cap_visits, total};
+  uint64_t nrounds = 1;
+
+  if (total > 0) {
+    const uint32_t scan_blocks = std::min<uint32_t>((total + 3) / 4, (uint32_t)ctx->num_sms * 16);
+    if (!rounds) {
+      ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, nullptr, 0);
+      DTB_CUDA(ctx, cudaGetLastError());
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3((unsigned)(ctx->num_sms * ctx->persist_blocks_per_sm[mode]));
+      cfg.blockDim = dim3(PERSIST_WPC * 32);
+      cfg.dynamicSmemBytes = PERSIST_SMEM;
+      cfg.stream = stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      if (mode == MODE_NS)
+        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
+      else
+        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
+    } else {
+      DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
+      ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, act0, 0);
+      DTB_CUDA(ctx, cudaGetLastError());
+      uint8_t* cur = act0;
+      uint8_t* nxt = act1;
+      uint32_t hchanged = 1;
+      nrounds = 0;
+      while (hchanged) {
+        DTB_CUDA(ctx, cudaMemsetAsync(nxt, 0, total, stream));
+        DTB_CUDA(ctx, cudaMemsetAsync(changed, 0, 4, stream));
+        const uint32_t blocks = (total + ROUND_WPC - 1) / ROUND_WPC;
+        if (mode == MODE_NS)
+          ggdt_round<MODE_NS, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
+        else
+          ggdt_round<MODE_REF, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
+        DTB_CUDA(ctx, cudaGetLastError());
+        DTB_CUDA(ctx, cudaMemcpyAsync(&hchanged, changed, 4, cudaMemcpyDeviceToHost, stream));
+        DTB_CUDA(ctx, cudaStreamSynchronize(stream));
+        std::swap(cur, nxt);
+        ++nrounds;
+        uint32_t err_prog[2] = {0, 0};
+        DTB_CUDA(ctx, cudaMemcpy(&err_prog[0], &hdr->error.v, 4, cudaMemcpyDeviceToHost));
+        DTB_CUDA(ctx, cudaMemcpy(&err_prog[1], &hdr->progress.v, 4, cudaMemcpyDeviceToHost));
+        if (err_prog[0]) break;
+        if (err_prog[1] > cap_visits) return fail(ctx, DTB_ERR_DEVICE, "visit limit exceeded after %llu rounds", (unsigned long long)nrounds);
+      }
+    }
+    ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states);
+    DTB_CUDA(ctx, cudaGetLastError());
+  }
+
+  // ---- copy staged outputs back ----
+  bool host_out = false;
+  for (auto& st : staged) {
+    if (!st.copy_out) continue;
+    const dtb_image* u = st.user;
+    const cudaMemcpyKind kind = u->memory_kind == DTB_CPU ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    host_out |= u->memory_kind == DTB_CPU;
+    DTB_CUDA(ctx, cudaMemcpy2DAsync(u->buffer, (size_t)u->pitch, st.dev, (size_t)st.pitch, (size_t)u->width * u->elem_size,
+                                    (size_t)u->height, kind, stream));
+  }
+  bool host_in = false;
+  for (auto& st : staged) host_in |= st.copy_in && st.user->memory_kind == DTB_CPU;
+
+  ctx->last_hdr = hdr;
+  ctx->last_tiles = total;
+  ctx->last_stream = stream;
+  ctx->stats = dtb_stats{};
+  ctx->stats.tiles = total;
+  ctx->stats.rounds = nrounds;
+  const bool async = (flags & DTB_FLAG_ASYNC) && !host_out && !host_in;
+  if (async) {
+    ctx->async_pending = true;
+    return DTB_OK;
+  }
+  ctx->async_pending = true;
+  return dtb_sync(ctx, stream);
+}
+
+}  // namespace dtb
+
+// ======================================================================================================
+// C ABI
+// ======================================================================================================
+extern "C" {
+
+DTB_API int32_t dtb_abi_version(void) { return DTB_ABI_VERSION; }
+
+DTB_API const char* dtb_status_string(dtb_status s) {
+  switch (s) {
+    case DTB_OK: return "ok";
+    case DTB_ERR_INVALID_ARG: return "invalid argument";
+    case DTB_ERR_CUDA: return "CUDA error";
+    case DTB_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case DTB_ERR_TIMEOUT: return "device wait timed out";
+    case DTB_ERR_DEVICE: return "device-side error";
+    case DTB_ERR_NO_DEVICE: return "no usable device";
+    case DTB_ERR_CAPACITY: return "capacity exceeded";
+  }
+  return "unknown status";
+}
+
+DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
+  if (!out) return DTB_ERR_INVALID_ARG;
+  *out = nullptr;
+  int dev = device;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return DTB_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return DTB_ERR_NO_DEVICE;
+  if (prop.major < 10) return DTB_ERR_NO_DEVICE;
+  if (cudaSetDevice(dev) != cudaSuccess) return DTB_ERR_NO_DEVICE;
+  dtb_context ctx = new (std::nothrow) dtb_context_s();
+  if (!ctx) return DTB_ERR_OUT_OF_MEMORY;
+  ctx->device = dev;
+  ctx->num_sms = prop.multiProcessorCount;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    delete ctx;
+    return DTB_ERR_NO_DEVICE;
+  }
+  ctx->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  const void* kp[2] = {(const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>,
+                        (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>};
+  const void* kr[2] = {(const void*)ggdt_round<MODE_NS, ROUND_WPC>, (const void*)ggdt_round<MODE_REF, ROUND_WPC>};
+  for (int m = 0; m < 2; ++m) {
+    if (cudaFuncSetAttribute(kp[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(kr[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROUND_SMEM) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->persist_blocks_per_sm[m], kp[m], PERSIST_WPC * 32,
+                                                      PERSIST_SMEM) != cudaSuccess ||
+        ctx->persist_blocks_per_sm[m] < 1) {
+      delete ctx;
+      return DTB_ERR_NO_DEVICE;
+    }
+  }
+  *out = ctx;
+  return DTB_OK;
+}
+
+DTB_API void dtb_context_destroy(dtb_context ctx) {
+  if (!ctx) return;
+  if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
+  if (ctx->dscratch) cudaFree(ctx->dscratch);
+  if (ctx->dstage) cudaFree(ctx->dstage);
+  delete ctx;
+}
+
+DTB_API const char* dtb_context_message(dtb_context ctx) { return ctx ? ctx->msg.c_str() : ""; }
+
+DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out) {
+  if (!ctx || !out) return DTB_ERR_INVALID_ARG;
+  *out = ctx->stats;
+  return DTB_OK;
+}
+
+DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  DTB_CUDA(ctx, cudaStreamSynchronize(st));
+  if (!ctx->async_pending) return DTB_OK;
+  ctx->async_pending = false;
+  QueueHdr h;
+  DTB_CUDA(ctx, cudaMemcpy(&h, ctx->last_hdr, sizeof(QueueHdr), cudaMemcpyDeviceToHost));
+  ctx->stats.tile_visits = h.progress.v;
+  ctx->stats.phases = h.phases.v;
+  ctx->stats.activations = h.activations.v;
+  ctx->stats.device_error = h.error.v;
+  ctx->stats.device_error_info = h.err_info.v;
+  switch (h.error.v) {
+    case DERR_NONE: return DTB_OK;
+    case DERR_QUEUE_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "tile queue made no progress within the time limit (ticket %u)", h.err_info.v);
+    case DERR_TMA_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "TMA transfer of tile %u did not complete", h.err_info.v);
+    case DERR_PHASE_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile %u did not converge within %d phases", h.err_info.v, PHASE_LIMIT);
+    case DERR_RING_FULL: return fail(ctx, DTB_ERR_DEVICE, "queue ring slot stayed occupied (tile %u)", h.err_info.v);
+    case DERR_VISIT_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile visit limit exceeded (%u)", h.err_info.v);
+    case DERR_BAD_TILE: return fail(ctx, DTB_ERR_DEVICE, "internal error: activation of tile %u outside the call", h.err_info.v);
+    default: return fail(ctx, DTB_ERR_DEVICE, "device error %u", h.error.v);
+  }
+}
+
+static dtb_status check_pair(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                             bool allow_rgb) {
+  dtb_status s;
+  if ((s = validate_view(ctx, img, "img", 1, allow_rgb ? 3 : 1)) != DTB_OK) return s;
+  if ((s = validate_view(ctx, mask, "mask", 1, 1)) != DTB_OK) return s;
+  if ((s = validate_view(ctx, dist, "dist", 4, 4)) != DTB_OK) return s;
+  if (img->width != mask->width || img->height != mask->height || img->width != dist->width || img->height != dist->height)
+    return fail(ctx, DTB_ERR_INVALID_ARG, "img, mask and dist must have the same size");
+  return DTB_OK;
+}
+
+static bool valid_v(float v) { return v >= 0.0f; }  // also rejects NaN
+
+DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                               float lambda, float v, uint32_t flags, void* stream) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->msg.clear();
+  dtb_status s = check_pair(ctx, img, mask, dist, false);
+  if (s != DTB_OK) return s;
+  if (!(lambda >= 0.0f && lambda <= 1.0f)) return fail(ctx, DTB_ERR_INVALID_ARG, "lambda must be in [0, 1]");
+  if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
+  DTB_CUDA(ctx, cudaSetDevice(ctx->device));
+  Job j = Job::from(img, mask, dist);
+  j.mode = MODE_REF;
+  j.v = v;
+  j.l_grad = lambda;
+  j.l_eucl = 1.0f - lambda;  // reference generalised_distance_transform.cu:108-109
+  j.ref_fma = (flags & DTB_FLAG_REF_NO_FMA) ? 0 : 1;
+  const dtb_image* a[1] = {img};
+  const dtb_image* b[1] = {mask};
+  const dtb_image* c[1] = {dist};
+  return run_jobs(ctx, {j}, a, b, c, flags, reinterpret_cast<cudaStream_t>(stream));
+}
+
+DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist, float gamma,
+                           float v, uint32_t flags, void* stream) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->msg.clear();
+  dtb_status s = check_pair(ctx, img, mask, dist, true);
+  if (s != DTB_OK) return s;
+  if (!(gamma >= 0.0f) || std::isinf(gamma)) return fail(ctx, DTB_ERR_INVALID_ARG, "gamma must be finite and >= 0");
+  if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
+  DTB_CUDA(ctx, cudaSetDevice(ctx->device));
+  Job j = Job::from(img, mask, dist);
+  j.mode = MODE_NS;
+  j.v = v;
+  j.g2 = gamma_to_g2(gamma);
+  const dtb_image* a[1] = {img};
+  const dtb_image* b[1] = {mask};
+  const dtb_image* c[1] = {dist};
+  return run_jobs(ctx, {j}, a, b, c, flags, reinterpret_cast<cudaStream_t>(stream));
+}
+
+DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
+                                 const dtb_image* dists, const float* gammas, float v, uint32_t flags, void* stream) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->msg.clear();
+  if (n < 0 || (n > 0 && (!imgs || !masks || !dists || !gammas))) return fail(ctx, DTB_ERR_INVALID_ARG, "bad batch arrays");
+  if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
+  std::vector<Job> jobs;
+  std::vector<const dtb_image*> a(n), b(n), c(n);
+  jobs.reserve(n);
+  for (int i = 0; i < n; ++i) {
+    dtb_status s = check_pair(ctx, &imgs[i], &masks[i], &dists[i], true);
+    if (s != DTB_OK) return fail(ctx, s, "image %d: %s", i, ctx->msg.c_str());
+    if (!(gammas[i] >= 0.0f) || std::isinf(gammas[i])) return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: bad gamma", i);
+    Job j = Job::from(&imgs[i], &masks[i], &dists[i]);
+    j.mode = MODE_NS;
+    j.v = v;
+    j.g2 = gamma_to_g2(gammas[i]);
+    jobs.push_back(j);
+    a[i] = &imgs[i];
+    b[i] = &masks[i];
+    c[i] = &dists[i];
+  }
+  DTB_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (flags & DTB_FLAG_ROUNDS) {
+    // Plain per-image path: one image after the other.
+    dtb_stats acc{};
+    for (int i = 0; i < n; ++i) {
+      dtb_status s = run_jobs(ctx, {jobs[i]}, &a[i], &b[i], &c[i], flags & ~DTB_FLAG_ASYNC, reinterpret_cast<cudaStream_t>(stream));
+      if (s != DTB_OK) return s;
+      acc.tiles += ctx->stats.tiles;
+      acc.tile_visits += ctx->stats.tile_visits;
+      acc.phases += ctx->stats.phases;
+      acc.activations += ctx->stats.activations;
+      acc.rounds += ctx->stats.rounds;
+    }
+    ctx->stats = acc;
+    return DTB_OK;
+  }
+  return run_jobs(ctx, jobs, a.data(), b.data(), c.data(), flags, reinterpret_cast<cudaStream_t>(stream));
+}
+
+static dtb_status copy2d(const dtb_image* src, const dtb_image* dst, cudaMemcpyKind kind, void* stream) {
+  if (!src || !dst) return DTB_ERR_INVALID_ARG;
+  if (src->width != dst->width || src->height != dst->height || src->elem_size != dst->elem_size) return DTB_ERR_INVALID_ARG;
+  if (src->width == 0 || src->height == 0) return DTB_OK;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpy2DAsync(dst->buffer, (size_t)dst->pitch, src->buffer, (size_t)src->pitch,
+                                    (size_t)src->width * src->elem_size, (size_t)src->height, kind, st);
+  if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? DTB_OK : DTB_ERR_CUDA;
+}
+
+DTB_API dtb_status dtb_host_to_device(const dtb_image* src, const dtb_image* dst, void* stream) {
+  if (!src || !dst || src->memory_kind != DTB_CPU || dst->memory_kind != DTB_GPU) return DTB_ERR_INVALID_ARG;
+  return copy2d(src, dst, cudaMemcpyHostToDevice, stream);
+}
+
+DTB_API dtb_status dtb_device_to_host(const dtb_image* src, const dtb_image* dst, void* stream) {
+  if (!src || !dst || src->memory_kind != DTB_GPU || dst->memory_kind != DTB_CPU) return DTB_ERR_INVALID_ARG;
+  return copy2d(src, dst, cudaMemcpyDeviceToHost, stream);
+}
+
+}  // extern "C"

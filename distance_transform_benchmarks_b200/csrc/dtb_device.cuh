@@ -1,0 +1,242 @@
+// dtb_device.cuh -- device-side building blocks of the B200 GGDT: tile states, the persistent tile queue,
+// TMA staging, edge weights, exact single-edge sweeps and the warp-per-tile visit.
+//
+// The computed map is the greatest fixpoint of single-edge relaxations D(p) <- min(D(p), relax(D(q), q->p))
+// from D = mask ? 0 : v (reference dt/src/utils.cu:12).  relax() is monotone in D(q), so any schedule that
+// runs to quiescence reaches the same fixpoint bit for bit; this is what lets a warp-per-tile schedule with
+// a device queue reproduce the reference's raster rounds (dt/src/generalised_distance_transform.cu:126-134)
+// exactly.  Every relaxation below is a single edge with the exact per-edge arithmetic; no step ever
+// combines two edge weights before adding them to a distance.
+#pragma once
+
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace dtb {
+
+constexpr int TILE = 32;                  // tile side (pixels); one warp owns one tile
+constexpr int IMG_BOX_ROWS = TILE + 2;    // image box rows: 1-pixel halo above and below
+constexpr int IMG_BOX_GRAY = 64;          // gray box width (bytes): x0-16 .. x0+47 covers x0-1 .. x0+32
+constexpr int IMG_BOX_RGB = 128;          // rgb8 box width (bytes): 3*x0-16 .. 3*x0+111 covers 3*(x0-1) .. 3*(x0+33)
+constexpr int S_STRIDE = TILE + 1;        // padded transpose buffer stride (floats): conflict-free both ways
+
+// Tile state word: flags in the low byte, image index of the tile in the upper 24 bits.
+constexpr uint32_t ST_PENDING = 1u;   // queued (or: re-run requested while running)
+constexpr uint32_t ST_RUNNING = 2u;   // a warp is visiting the tile
+constexpr uint32_t ST_VISITED = 4u;   // the tile's distances in global memory are valid
+constexpr uint32_t ST_SEED = 8u;      // the next visit applies the seed mask of the tile
+constexpr int ST_IMG_SHIFT = 8;
+
+// Weight modes.
+constexpr int32_t MODE_NS = 0;   // C4, w = sqrt(1 + g2 * dI2), gray or rgb8
+constexpr int32_t MODE_REF = 1;  // C8, D(q) + l_eucl * {1, sqrt2} + l_grad * |dI|, gray (reference weight)
+
+// Device error codes (written once into Queue::error).
+constexpr uint32_t DERR_NONE = 0;
+constexpr uint32_t DERR_QUEUE_TIMEOUT = 1;   // no global progress for the configured time
+constexpr uint32_t DERR_TMA_TIMEOUT = 2;     // a TMA transaction did not complete in time
+constexpr uint32_t DERR_PHASE_LIMIT = 3;     // a tile did not converge within the phase limit
+constexpr uint32_t DERR_RING_FULL = 4;       // a ring slot stayed occupied
+constexpr uint32_t DERR_VISIT_LIMIT = 5;     // more tile visits than the call's cap (a safety net)
+constexpr uint32_t DERR_BAD_TILE = 6;        // an activation named a tile outside the call (internal bug)
+
+// One image of a (possibly ragged) batch.  Pitches are in bytes.
+struct alignas(64) ImgDesc {
+  const uint8_t* img;
+  const uint8_t* mask;
+  float* dist;
+  int64_t img_pitch;
+  int64_t mask_pitch;
+  int64_t dist_pitch;
+  int32_t width, height, channels, tiles_x, tiles_y;
+  uint32_t tile_base;
+  float g2;       // ns-mode: fl32(gamma * gamma)
+  float v;        // value of unreached pixels (>= 0)
+  float l_eucl;   // ref-mode: 1 - lambda
+  float l_grad;   // ref-mode: lambda
+  int32_t mode;
+  int32_t ref_fma;  // ref-mode: 1 = fma(l_grad, dI, fma(l_eucl, d, D)), 0 = left-to-right rounding
+};
+
+// Counters live on separate 128-byte lines.
+struct alignas(128) Line { uint32_t v; uint32_t pad[31]; };
+struct QueueHdr {
+  Line head;       // next pop ticket
+  Line tail;       // next push position
+  Line pending;    // tiles queued or running
+  Line error;      // first device error code
+  Line progress;   // completed visits (used by the no-progress watchdog)
+  Line phases;     // total sweep phases
+  Line activations;  // neighbour activations issued
+  Line err_info;   // tile id / detail of the first error
+};
+
+struct Queue {
+  QueueHdr* hdr;
+  uint32_t* ring;
+  uint32_t mask;            // ring capacity - 1 (capacity is a power of two)
+  uint64_t timeout_ns;      // watchdog: give up after this long without any completed visit
+  uint32_t max_visits;      // safety net against endless re-activation
+  uint32_t total_tiles;     // tile ids are < total_tiles
+};
+
+// Per-warp shared memory slot.
+struct alignas(128) WarpSmem {
+  uint8_t img[IMG_BOX_ROWS * IMG_BOX_RGB];   // TMA destination (gray uses IMG_BOX_ROWS x 64)
+  uint8_t mask[TILE * TILE];                 // TMA destination for seed masks
+  float S[TILE * S_STRIDE];                  // transpose / final tile values
+  float er[TILE];                            // weights of the edges x=31 -> x=32 per row
+  float hl[TILE + 2];                        // ref-mode: halo column x = -1 (rows -1..32)
+  float hr[TILE + 2];                        // ref-mode: halo column x = 32
+  uint64_t bar;                              // TMA mbarrier
+};
+
+// ------------------------------------------------------------------------------------------------------
+// PTX helpers
+// ------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 2-D tiled TMA load into this CTA's shared memory.  The innermost coordinate x must be a multiple of 16
+// bytes / element size; every call site below passes x0 - 16, 3*x0 - 16 (gray/rgb8 boxes) or x0, with x0 a
+// multiple of 32.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Queue: a ticket ring of tile ids with a pending counter for termination.
+//   push: pending += 1, then a tail ticket, then the item into its slot (slot must be free: CAS from 0).
+//   pop:  a head ticket, then wait until its slot holds an item, or until pending == 0 (done), or error.
+// Items are interchangeable, so a popper that takes an item meant for another ticket of the same slot is
+// harmless: every item is taken exactly once (atomicExch) and no slot is written twice (CAS from 0).
+// All waits are bounded by a no-global-progress watchdog and end with an error code, never a hang.
+// ------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void set_error(const Queue& q, uint32_t code, uint32_t info) {
+  if (atomicCAS(&q.hdr->error.v, 0u, code) == 0u) atomicExch(&q.hdr->err_info.v, info);
+}
+
+__device__ __forceinline__ void queue_push(const Queue& q, uint32_t item) {
+  atomicAdd(&q.hdr->pending.v, 1u);
+  const uint32_t p = atomicAdd(&q.hdr->tail.v, 1u);
+  uint32_t* slot = &q.ring[p & q.mask];
+  uint32_t ns = 32;
+  const uint64_t t0 = globaltimer();
+  while (atomicCAS(slot, 0u, item + 1u) != 0u) {
+    if (globaltimer() - t0 > q.timeout_ns) { set_error(q, DERR_RING_FULL, item); atomicSub(&q.hdr->pending.v, 1u); return; }
+    __nanosleep(ns);
+    ns = ns < 1024 ? ns * 2 : ns;
+  }
+}
+
+constexpr uint32_t POP_NONE = 0xFFFFFFFFu;
+
+// Called by one lane.  Returns a tile id or POP_NONE (queue drained, or error).
+__device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
+  const uint32_t h = atomicAdd(&q.hdr->head.v, 1u);
+  uint32_t* slot = &q.ring[h & q.mask];
+  uint32_t ns = 16;
+  uint64_t t0 = 0;
+  uint32_t seen = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (ld_volatile(slot) != 0u) {
+      const uint32_t v = atomicExch(slot, 0u);
+      if (v != 0u) {
+        if (ld_volatile(&q.hdr->progress.v) > q.max_visits) {
+          set_error(q, DERR_VISIT_LIMIT, v - 1u);
+          return POP_NONE;  // the item is dropped: the call has failed anyway
+        }
+        return v - 1u;
+      }
+    }
+    if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;
+    if (ld_volatile(&q.hdr->error.v) != 0u) return POP_NONE;
+    if ((it & 15u) == 0u) {
+      const uint32_t prog = ld_volatile(&q.hdr->progress.v);
+      if (prog > q.max_visits) { set_error(q, DERR_VISIT_LIMIT, prog); return POP_NONE; }
+      const uint64_t now = globaltimer();
+      if (it == 0 || prog != seen) { seen = prog; t0 = now; }
+      else if (now - t0 > q.timeout_ns) { set_error(q, DERR_QUEUE_TIMEOUT, h); return POP_NONE; }
+    }
+    __nanosleep(ns);
+    ns = ns < 512 ? ns * 2 : ns;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Edge weights
+// ------------------------------------------------------------------------------------------------------
+// ns-mode: w = sqrt(1 + g2 * dI2), dI2 = sum_c (I_c(p) - I_c(q))^2.  Pixels are packed little-endian in a
+// u32 (gray: byte 0; rgb8: bytes 0..2), unused bytes zero.  dI2 <= 3 * 255^2 is exact in fp32; each of the
+// three float operations is rounded separately (no contraction), the square root correctly rounded.
+__device__ __forceinline__ float ns_weight(uint32_t pa, uint32_t pb, float g2) {
+  const uint32_t ad = __vabsdiffu4(pa, pb);
+  const uint32_t dI2 = __dp4a(ad, ad, 0u);
+  return __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(g2, __uint2float_rn(dI2))));
+}
+
+// ref-mode relaxation of one edge, reference dt/src/dt_block_passes.cuh:252-253:
+//   D(q) + l_eucl * local_dist2d[k] + l_grad * |I(p) - I(q)|
+template <bool FMA>
+__device__ __forceinline__ float ref_relax(float dq, float eucl_d, float l_eucl, float l_grad, float absdi) {
+  if (FMA) return __fmaf_rn(l_grad, absdi, __fmaf_rn(l_eucl, eucl_d, dq));
+  return __fadd_rn(__fadd_rn(dq, __fmul_rn(l_eucl, eucl_d)), __fmul_rn(l_grad, absdi));
+}
+
+// ------------------------------------------------------------------------------------------------------
+// One phase along a line of 32 pixels held in registers: a forward chain from `lo` (the halo before
+// d[0]) and a backward chain from `hi` (the halo after d[31]), interleaved for two independent dependency
+// chains.  w[k] is the weight of the edge between positions k-1 and k (w[0]: lo -> d[0], w[32]: d[31] ->
+// hi).  Each step is one single-edge relaxation fl(D + w); after the phase every edge of the line is
+// satisfied in both directions.  Returns whether any value decreased.
+// ------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool sweep_line(float (&d)[TILE], const float (&w)[TILE + 1], float lo, float hi) {
+  bool ch = false;
+  float f = lo, b = hi;
+#pragma unroll
+  for (int k = 0; k < TILE; ++k) {
+    const int yf = k, yb = TILE - 1 - k;
+    const float t = __fadd_rn(f, w[yf]);
+    ch |= t < d[yf];
+    d[yf] = fminf(d[yf], t);
+    f = d[yf];
+    const float u = __fadd_rn(b, w[yb + 1]);
+    ch |= u < d[yb];
+    d[yb] = fminf(d[yb], u);
+    b = d[yb];
+  }
+  return ch;
+}
+
+}  // namespace dtb

@@ -1,0 +1,582 @@
+// dtb_kernels.cuh -- the GGDT tile visit (warp per 32x32 tile) and the kernels built from it.
+//
+// Kernels
+//   ggdt_scan        seed-tile scan: reads every mask tile once, writes the tile states and queues the tiles
+//                    that hold seeds (replaces initialize_generalised_distance_map + initialize_task_queue,
+//                    reference dt/src/utils.cu:5-18, and the priority set-up of dt/src/block_priority.cu).
+//   ggdt_persistent  cooperative persistent kernel: every warp pops tiles from the shared queue, visits them
+//                    and re-activates neighbours whose halo it can still lower (replaces the task variant,
+//                    reference dt/src/generalised_distance_transform_task.cu:129-150).  No grid barrier:
+//                    termination is "queue empty and nothing in flight".
+//   ggdt_round       one host-driven round over the active tiles (the plain per-image path; the round
+//                    structure of reference dt/src/generalised_distance_transform_blocks.cu:156-163).
+//   ggdt_finalize    writes v into tiles that were never reached (their memory was never initialised).
+#pragma once
+
+#include "dtb_device.cuh"
+
+namespace dtb {
+
+constexpr int PHASE_LIMIT = 4096;
+constexpr uint64_t TMA_TIMEOUT_NS = 2000000000ull;  // 2 s
+
+// ------------------------------------------------------------------------------------------------------
+// Schedulers: what "activate a neighbour" and "finish a visit" mean.
+// ------------------------------------------------------------------------------------------------------
+struct QueueSched {
+  Queue q;
+  uint32_t* states;
+  // Idle -> queued; running -> running + re-run requested; queued -> unchanged.
+  __device__ __forceinline__ void activate(uint32_t tile) const {
+    if (tile >= q.total_tiles) { set_error(q, DERR_BAD_TILE, tile); return; }
+    const uint32_t old = atomicOr(&states[tile], ST_PENDING);
+    if (!(old & (ST_PENDING | ST_RUNNING))) queue_push(q, tile);
+  }
+  __device__ __forceinline__ void finish(uint32_t tile, uint32_t xor_bits, uint32_t nphase, uint32_t nact) const {
+    const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
+    if (old & ST_PENDING) queue_push(q, tile);  // a neighbour asked for a re-run while this visit ran
+    atomicAdd(&q.hdr->phases.v, nphase);
+    if (nact) atomicAdd(&q.hdr->activations.v, nact);
+    atomicAdd(&q.hdr->progress.v, 1u);
+    atomicSub(&q.hdr->pending.v, 1u);
+  }
+};
+
+struct RoundSched {
+  Queue q;  // only the counters and error word are used
+  uint32_t* states;
+  uint8_t* next_active;
+  uint32_t* changed;
+  __device__ __forceinline__ void activate(uint32_t tile) const {
+    if (tile >= q.total_tiles) { set_error(q, DERR_BAD_TILE, tile); return; }
+    next_active[tile] = 1;
+    *(volatile uint32_t*)changed = 1u;
+  }
+  __device__ __forceinline__ void finish(uint32_t tile, uint32_t xor_bits, uint32_t nphase, uint32_t nact) const {
+    if (xor_bits) atomicXor(&states[tile], xor_bits);
+    atomicAdd(&q.hdr->phases.v, nphase);
+    if (nact) atomicAdd(&q.hdr->activations.v, nact);
+    atomicAdd(&q.hdr->progress.v, 1u);
+  }
+};
+
+__device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
+
+__device__ __forceinline__ float* dist_row(const ImgDesc& dd, int y) {
+  return reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(dd.dist) + (int64_t)y * dd.dist_pitch);
+}
+
+// Waits for the TMA transactions of this warp's slot.  Bounded: on timeout the error word is set and the
+// wait goes on (bounded again) so that no copy is left in flight when the warp leaves.
+__device__ __forceinline__ bool tma_wait(WarpSmem& sm, uint32_t& parity, const Queue& q, uint32_t tile) {
+  const uint64_t t0 = globaltimer();
+  bool ok = true;
+  while (!mbar_try_wait(&sm.bar, parity)) {
+    const uint64_t dt = globaltimer() - t0;
+    if (ok && dt > TMA_TIMEOUT_NS) { set_error(q, DERR_TMA_TIMEOUT, tile); ok = false; }
+    if (dt > 2 * TMA_TIMEOUT_NS) break;
+  }
+  parity ^= 1u;
+  return ok;
+}
+
+// Stages the image box (with 1-pixel halo) and, if needed, the seed-mask tile of a tile into shared memory.
+__device__ __forceinline__ void stage_tile(WarpSmem& sm, const CUtensorMap* tm_img, const CUtensorMap* tm_mask, bool rgb,
+                                           bool with_mask, int x0, int y0) {
+  // Order this warp's earlier generic reads of the slot before the async-proxy writes below.
+  fence_proxy_async_smem();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    tmap_acquire(tm_img);
+    if (with_mask) tmap_acquire(tm_mask);
+    const uint32_t bytes = (rgb ? IMG_BOX_RGB : IMG_BOX_GRAY) * IMG_BOX_ROWS + (with_mask ? TILE * TILE : 0);
+    mbar_arrive_expect_tx(&sm.bar, bytes);
+    tma_load_2d(sm.img, tm_img, rgb ? 3 * x0 - 16 : x0 - 16, y0 - 1, &sm.bar);
+    if (with_mask) tma_load_2d(sm.mask, tm_mask, x0, y0, &sm.bar);
+  }
+}
+
+// Packed pixel of the staged image box: box row r (tile row r - 1), tile column c in [-1, 32].
+__device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r, int c) {
+  if (!rgb) return box[r * IMG_BOX_GRAY + 16 + c];
+  const int off = r * IMG_BOX_RGB + 16 + 3 * c;
+  const uint32_t* wp = reinterpret_cast<const uint32_t*>(box + (off & ~3));
+  return __funnelshift_r(wp[0], wp[1], (off & 3) * 8) & 0xFFFFFFu;
+}
+
+// ------------------------------------------------------------------------------------------------------
+// ns-mode visit (C4, w = sqrt(1 + g2 * dI2)), gray or rgb8.
+//
+// Layouts: "column" (lane = x, d[y]) and "row" (lane = y, d[x]).  A phase relaxes every edge of one
+// orientation with the two interleaved chains of sweep_line; the tile switches layout through the padded
+// buffer S.  The visit stops after a phase that changed nothing (and at least two phases), at which point
+// every edge of the tile and its halo is satisfied.  The halo is an upper bound of the neighbours' values
+// (values only decrease), so the visit never undershoots the fixpoint.  A neighbour is re-activated only if
+// some border pixel plus its edge weight is below the halo value it was compared against: the neighbour can
+// then still decrease; otherwise it cannot (its value is <= that halo value).
+// ------------------------------------------------------------------------------------------------------
+template <class Sched>
+__device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
+                                         uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
+                                         const Sched& sch) {
+  const int lane = threadIdx.x & 31;
+  const float INF = f_inf();
+  const uint32_t local = tile - dd.tile_base;
+  const int tx = (int)(local % (uint32_t)dd.tiles_x), ty = (int)(local / (uint32_t)dd.tiles_x);
+  const int x0 = tx * TILE, y0 = ty * TILE;
+  const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
+  const bool first = !(old_state & ST_VISITED);
+  const bool seed = (old_state & ST_SEED) != 0;
+  const bool rgb = dd.channels == 3;
+  const float v = dd.v;
+
+  stage_tile(sm, tm_img, tm_mask, rgb, seed, x0, y0);
+
+  // Neighbour states: lane 0 left, 1 right, 2 top, 3 bottom.
+  uint32_t nvis;
+  {
+    bool vis = false;
+    if (lane < 4) {
+      const int nx = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
+      const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
+      if (nx >= 0 && ny >= 0 && nx < dd.tiles_x && ny < dd.tiles_y)
+        vis = (ld_volatile(&sch.states[dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx)]) & ST_VISITED) != 0;
+    }
+    nvis = __ballot_sync(~0u, vis);
+  }
+  __threadfence();  // acquire: distances were written before the VISITED bits / the activation we saw
+
+  // Halo: column layout for top/bottom (lane = x), row layout for left/right (lane = y).
+  float top = INF, bot = INF, lft = INF, rgt = INF;
+  if (lane < vw) {
+    if (ty > 0) top = (nvis & 4u) ? dist_row(dd, y0 - 1)[x0 + lane] : v;
+    if (ty + 1 < dd.tiles_y) bot = (nvis & 8u) ? dist_row(dd, y0 + TILE)[x0 + lane] : v;
+  }
+  if (lane < vh) {
+    if (tx > 0) lft = (nvis & 1u) ? dist_row(dd, y0 + lane)[x0 - 1] : v;
+    if (tx + 1 < dd.tiles_x) rgt = (nvis & 2u) ? dist_row(dd, y0 + lane)[x0 + TILE] : v;
+  }
+
+  // Tile distances in column layout.
+  float d[TILE];
+  if (!first) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? dist_row(dd, y0 + y)[x0 + lane] : INF;
+  }
+
+  if (!tma_wait(sm, parity, sch.q, tile)) return;
+
+  // Edge weights.  wv[k]: edge (row k-1, row k) of column `lane`; horizontal weights go through S.
+  const float g2 = dd.g2;
+  float wv[TILE + 1];
+  {
+    const uint8_t* box = sm.img;
+    uint32_t pprev = box_pix(box, rgb, 0, lane);
+#pragma unroll
+    for (int r = 1; r <= TILE + 1; ++r) {
+      const uint32_t pcur = box_pix(box, rgb, r, lane);
+      wv[r - 1] = ns_weight(pprev, pcur, g2);
+      if (r <= TILE) sm.S[(r - 1) * S_STRIDE + lane] = ns_weight(box_pix(box, rgb, r, lane - 1), pcur, g2);
+      pprev = pcur;
+    }
+  }
+  // Edge (x = 31, x = 32) of row `lane`.
+  const float er = ns_weight(box_pix(sm.img, rgb, lane + 1, TILE - 1), box_pix(sm.img, rgb, lane + 1, TILE), g2);
+#pragma unroll
+  for (int k = 0; k <= TILE; ++k)
+    if (lane >= vw || (k < TILE ? k >= vh : TILE - 1 >= vh)) wv[k] = INF;
+  __syncwarp();
+  float wh[TILE + 1];
+#pragma unroll
+  for (int k = 0; k < TILE; ++k) wh[k] = sm.S[lane * S_STRIDE + k];
+  wh[TILE] = er;
+#pragma unroll
+  for (int k = 0; k <= TILE; ++k)
+    if (lane >= vh || (k < TILE ? k >= vw : TILE - 1 >= vw)) wh[k] = INF;
+  __syncwarp();
+
+  if (first) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) {
+      const bool in = lane < vw && y < vh;
+      const bool s = seed && sm.mask[y * TILE + lane] != 0;
+      d[y] = in ? (s ? 0.0f : v) : INF;
+    }
+  } else if (seed) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y)
+      if (lane < vw && y < vh && sm.mask[y * TILE + lane] != 0) d[y] = 0.0f;
+  }
+
+  // Local fixpoint.
+  bool any = false;
+  uint32_t nph = 0;
+  bool col = true;
+  for (;;) {
+    bool ch = col ? sweep_line(d, wv, top, bot) : sweep_line(d, wh, lft, rgt);
+    ch = __any_sync(~0u, ch);
+    any |= ch;
+    ++nph;
+    if (col) {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = d[y];
+    } else {
+#pragma unroll
+      for (int x = 0; x < TILE; ++x) sm.S[lane * S_STRIDE + x] = d[x];
+    }
+    __syncwarp();
+    if ((!ch && nph >= 2) || nph >= (uint32_t)PHASE_LIMIT) break;
+    if (col) {
+#pragma unroll
+      for (int x = 0; x < TILE; ++x) d[x] = sm.S[lane * S_STRIDE + x];
+    } else {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y) d[y] = sm.S[y * S_STRIDE + lane];
+    }
+    col = !col;
+    __syncwarp();
+  }
+  if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);
+
+  // Neighbours that can still decrease (bit 0 left, 1 right, 2 top, 3 bottom).
+  uint32_t act = 0;
+  if (any || seed) {
+    const float dt = sm.S[lane], db = sm.S[(TILE - 1) * S_STRIDE + lane];
+    const float dl = sm.S[lane * S_STRIDE], dr = sm.S[lane * S_STRIDE + TILE - 1];
+    act |= __any_sync(~0u, __fadd_rn(dl, wh[0]) < lft) ? 1u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dr, wh[TILE]) < rgt) ? 2u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dt, wv[0]) < top) ? 4u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(db, wv[TILE]) < bot) ? 8u : 0u;
+    // A missing neighbour has an INF halo, and fl(d + w) < INF holds for any finite d: mask by existence.
+    const uint32_t nexist = (tx > 0 ? 1u : 0u) | (tx + 1 < dd.tiles_x ? 2u : 0u) | (ty > 0 ? 4u : 0u) |
+                            (ty + 1 < dd.tiles_y ? 8u : 0u);
+    act &= nexist;
+  }
+
+  // Write back (column layout: each row is one coalesced 128-byte store).
+  if (any || first) {
+    if (lane < vw) {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y)
+        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = sm.S[y * S_STRIDE + lane];
+    }
+  }
+  __threadfence();  // release: distances before activations and before the VISITED bit
+  __syncwarp();
+  if (lane < 4 && ((act >> lane) & 1u)) {
+    const int nx = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
+    const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
+    sch.activate(dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx));
+  }
+  __syncwarp();
+  if (lane == 0)
+    sch.finish(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), nph, (uint32_t)__popc(act));
+}
+
+// ------------------------------------------------------------------------------------------------------
+// ref-mode visit (C8, reference weight), gray only.
+//
+// Mirrors the reference's in-tile passes (dt/src/dt_block_passes.cuh:12-127): a row phase relaxes every
+// pixel from its three predecessors in the previous column (forward then backward), a column phase from
+// the three predecessors in the previous row.  The three rows (columns) move in lockstep, so the
+// predecessors of lane l come from lanes l-1 / l+1 by shuffle, or from the halo for the edge lanes.
+// Each relaxation is a single edge with the reference's arithmetic (ref_relax).  Neighbours (8 of them)
+// are re-activated when a border pixel facing them decreased, as in dt_block_passes.cuh:50-63, and on
+// visits that applied seeds.
+// ------------------------------------------------------------------------------------------------------
+constexpr int PIMG_STRIDE = 36;  // padded image copy: 34 rows x 36 bytes (odd word stride)
+
+template <bool FMA>
+__device__ __forceinline__ float ref_min3(float cur, float da, float db, float dc, float le, float lg, float sq2,
+                                          float ia, float ib, float ic, bool diag_a, bool diag_c) {
+  // a and c are the diagonal predecessors, b the axial one
+  const float ra = ref_relax<FMA>(da, diag_a ? sq2 : 1.0f, le, lg, ia);
+  const float rb = ref_relax<FMA>(db, 1.0f, le, lg, ib);
+  const float rc = ref_relax<FMA>(dc, diag_c ? sq2 : 1.0f, le, lg, ic);
+  return fminf(cur, fminf(rb, fminf(ra, rc)));
+}
+
+template <bool FMA, class Sched>
+__device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
+                                          uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
+                                          const Sched& sch) {
+  const int lane = threadIdx.x & 31;
+  const float INF = f_inf();
+  const uint32_t local = tile - dd.tile_base;
+  const int tx = (int)(local % (uint32_t)dd.tiles_x), ty = (int)(local / (uint32_t)dd.tiles_x);
+  const int x0 = tx * TILE, y0 = ty * TILE;
+  const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
+  const bool first = !(old_state & ST_VISITED);
+  const bool seed = (old_state & ST_SEED) != 0;
+  const float v = dd.v, le = dd.l_eucl, lg = dd.l_grad;
+  const float sq2 = 1.41421354f;  // sqrtf(2.f), reference generalised_distance_transform.cu:111
+
+  stage_tile(sm, tm_img, tm_mask, false, seed, x0, y0);
+
+  // Neighbour k = lane (0..7): (dx, dy) = L, R, T, B, TL, TR, BL, BR.
+  const int ndx[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
+  const int ndy[8] = {0, 0, -1, 1, -1, -1, 1, 1};
+  uint32_t nvis, nexist;
+  {
+    bool vis = false, ex = false;
+    if (lane < 8) {
+      const int nx = tx + ndx[lane], ny = ty + ndy[lane];
+      ex = nx >= 0 && ny >= 0 && nx < dd.tiles_x && ny < dd.tiles_y;
+      if (ex) vis = (ld_volatile(&sch.states[dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx)]) & ST_VISITED) != 0;
+    }
+    nvis = __ballot_sync(~0u, vis);
+    nexist = __ballot_sync(~0u, ex);
+  }
+  __threadfence();
+
+  // Halo rows / columns in shared memory, index = coordinate + 1 (corners appear in both).
+  float* ht = sm.S;                 // top row   (y0 - 1), x = -1..32
+  float* hb = sm.S + 40;            // bottom row (y0 + 32)
+  float* hl = sm.hl;                // left column (x0 - 1), y = -1..32
+  float* hr = sm.hr;                // right column (x0 + 32)
+  auto halo_val = [&](int k, int gx, int gy) -> float {  // neighbour k's pixel (gx, gy)
+    if (!((nexist >> k) & 1u)) return INF;
+    if (gx >= dd.width || gy >= dd.height) return INF;
+    return ((nvis >> k) & 1u) ? dist_row(dd, gy)[gx] : v;
+  };
+  ht[lane + 1] = (lane < vw) ? halo_val(2, x0 + lane, y0 - 1) : INF;
+  hb[lane + 1] = (lane < vw) ? halo_val(3, x0 + lane, y0 + TILE) : INF;
+  hl[lane + 1] = (lane < vh) ? halo_val(0, x0 - 1, y0 + lane) : INF;
+  hr[lane + 1] = (lane < vh) ? halo_val(1, x0 + TILE, y0 + lane) : INF;
+  if (lane == 0) {
+    const float tl = halo_val(4, x0 - 1, y0 - 1), tr = halo_val(5, x0 + TILE, y0 - 1);
+    const float bl = halo_val(6, x0 - 1, y0 + TILE), br = halo_val(7, x0 + TILE, y0 + TILE);
+    ht[0] = tl; hl[0] = tl;
+    ht[TILE + 1] = tr; hr[0] = tr;
+    hb[0] = bl; hl[TILE + 1] = bl;
+    hb[TILE + 1] = br; hr[TILE + 1] = br;
+  }
+
+  float d[TILE];
+  if (!first) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? dist_row(dd, y0 + y)[x0 + lane] : INF;
+  }
+
+  if (!tma_wait(sm, parity, sch.q, tile)) return;
+
+  // Padded copy of the image box: pimg[r * 36 + c + 1] = pixel (tile column c, box row r), c = -1..32.
+  uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.S + 96);  // 34 * 36 = 1224 bytes after the halo rows
+  for (int i = lane; i < IMG_BOX_ROWS * PIMG_STRIDE; i += 32) {
+    const int r = i / PIMG_STRIDE, c = i % PIMG_STRIDE;
+    pimg[i] = (c < TILE + 2) ? sm.img[r * IMG_BOX_GRAY + 15 + c] : 0;
+  }
+
+  if (first) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) {
+      const bool in = lane < vw && y < vh;
+      d[y] = in ? ((seed && sm.mask[y * TILE + lane] != 0) ? 0.0f : v) : INF;
+    }
+  } else if (seed) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y)
+      if (lane < vw && y < vh && sm.mask[y * TILE + lane] != 0) d[y] = 0.0f;
+  }
+  __syncwarp();
+
+  // Tile values live in T (column-layout transposes) = sm.img region after staging is consumed:
+  // the image is needed through pimg only from here on.
+  float* T = reinterpret_cast<float*>(sm.img);  // 32 x 33 floats = 4224 bytes <= 4352
+  // Initial border values for the change test.
+  const float it0 = d[0], ib0 = d[TILE - 1];
+#pragma unroll
+  for (int y = 0; y < TILE; ++y) T[y * S_STRIDE + lane] = d[y];
+  __syncwarp();
+  const float il0 = T[lane * S_STRIDE], ir0 = T[lane * S_STRIDE + TILE - 1];
+  __syncwarp();
+
+  auto P = [&](int r, int c) -> float {  // pixel at tile (c, r) as float, r, c in [-1, 32]
+    return (float)pimg[(r + 1) * PIMG_STRIDE + c + 1];
+  };
+  auto absd = [](float a, float b) { return fabsf(a - b); };  // exact for integers in [0, 255]
+
+  bool any = false;
+  uint32_t nph = 0;
+  bool col = true;
+  for (;;) {
+    bool ch = false;
+    if (col) {
+      // Column phase (lane = x): forward over y with predecessors (x-1..x+1, y-1), then backward.
+      const int x = lane;
+      const bool xin = lane < vw;
+#pragma unroll
+      for (int y = 0; y < TILE; ++y) {
+        float pa, pb, pc;
+        if (y == 0) { pa = ht[x]; pb = ht[x + 1]; pc = ht[x + 2]; }
+        else {
+          pb = d[y - 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = hl[y];
+          if (lane == TILE - 1) pc = hr[y];
+        }
+        const float c = P(y, x);
+        const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y - 1, x)),
+                                       absd(c, P(y - 1, x + 1)), true, true);
+        const bool upd = xin && y < vh && nd < d[y];
+        ch |= upd;
+        d[y] = upd ? nd : d[y];
+      }
+#pragma unroll
+      for (int y = TILE - 1; y >= 0; --y) {
+        float pa, pb, pc;
+        if (y == TILE - 1) { pa = hb[x]; pb = hb[x + 1]; pc = hb[x + 2]; }
+        else {
+          pb = d[y + 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = hl[y + 2];
+          if (lane == TILE - 1) pc = hr[y + 2];
+        }
+        const float c = P(y, x);
+        const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y + 1, x - 1)), absd(c, P(y + 1, x)),
+                                       absd(c, P(y + 1, x + 1)), true, true);
+        const bool upd = xin && y < vh && nd < d[y];
+        ch |= upd;
+        d[y] = upd ? nd : d[y];
+      }
+    } else {
+      // Row phase (lane = y): forward over x with predecessors (x-1, y-1..y+1), then backward.
+      const int y = lane;
+      const bool yin = lane < vh;
+#pragma unroll
+      for (int x = 0; x < TILE; ++x) {
+        float pa, pb, pc;
+        if (x == 0) { pa = hl[y]; pb = hl[y + 1]; pc = hl[y + 2]; }
+        else {
+          pb = d[x - 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = ht[x];
+          if (lane == TILE - 1) pc = hb[x];
+        }
+        const float c = P(y, x);
+        const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y, x - 1)),
+                                       absd(c, P(y + 1, x - 1)), true, true);
+        const bool upd = yin && x < vw && nd < d[x];
+        ch |= upd;
+        d[x] = upd ? nd : d[x];
+      }
+#pragma unroll
+      for (int x = TILE - 1; x >= 0; --x) {
+        float pa, pb, pc;
+        if (x == TILE - 1) { pa = hr[y]; pb = hr[y + 1]; pc = hr[y + 2]; }
+        else {
+          pb = d[x + 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = ht[x + 2];
+          if (lane == TILE - 1) pc = hb[x + 2];
+        }
+        const float c = P(y, x);
+        const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x + 1)), absd(c, P(y, x + 1)),
+                                       absd(c, P(y + 1, x + 1)), true, true);
+        const bool upd = yin && x < vw && nd < d[x];
+        ch |= upd;
+        d[x] = upd ? nd : d[x];
+      }
+    }
+    ch = __any_sync(~0u, ch);
+    any |= ch;
+    ++nph;
+    if (col) {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y) T[y * S_STRIDE + lane] = d[y];
+    } else {
+#pragma unroll
+      for (int x = 0; x < TILE; ++x) T[lane * S_STRIDE + x] = d[x];
+    }
+    __syncwarp();
+    if ((!ch && nph >= 2) || nph >= (uint32_t)PHASE_LIMIT) break;
+    if (col) {
+#pragma unroll
+      for (int x = 0; x < TILE; ++x) d[x] = T[lane * S_STRIDE + x];
+    } else {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y) d[y] = T[y * S_STRIDE + lane];
+    }
+    col = !col;
+    __syncwarp();
+  }
+  if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);
+
+  // Border changes -> neighbours (bit k = neighbour k as in ndx/ndy).
+  uint32_t act = 0;
+  if (any || seed) {
+    const bool force = seed;
+    const uint32_t ct = __ballot_sync(~0u, force || T[lane] != it0);
+    const uint32_t cb = __ballot_sync(~0u, force || T[(TILE - 1) * S_STRIDE + lane] != ib0);
+    const uint32_t cl = __ballot_sync(~0u, force || T[lane * S_STRIDE] != il0);
+    const uint32_t cr = __ballot_sync(~0u, force || T[lane * S_STRIDE + TILE - 1] != ir0);
+    act |= cl ? 1u : 0u;
+    act |= cr ? 2u : 0u;
+    act |= ct ? 4u : 0u;
+    act |= cb ? 8u : 0u;
+    act |= (ct & 1u) ? 16u : 0u;
+    act |= (ct >> (TILE - 1)) & 1u ? 32u : 0u;
+    act |= (cb & 1u) ? 64u : 0u;
+    act |= (cb >> (TILE - 1)) & 1u ? 128u : 0u;
+    act &= nexist;
+  }
+
+  if (any || first) {
+    if (lane < vw) {
+#pragma unroll
+      for (int y = 0; y < TILE; ++y)
+        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = T[y * S_STRIDE + lane];
+    }
+  }
+  __threadfence();
+  __syncwarp();
+  if (lane < 8 && ((act >> lane) & 1u))
+    sch.activate(dd.tile_base + (uint32_t)((ty + ndy[lane]) * dd.tiles_x + tx + ndx[lane]));
+  __syncwarp();
+  if (lane == 0)
+    sch.finish(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), nph, (uint32_t)__popc(act));
+}
+
+// MODE is fixed per kernel instantiation: a launch covers images of one weight mode only, so the
+// register allocation of the ns-mode kernel is not inflated by the ref-mode code.
+template <int MODE, class Sched>
+__device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap* tmaps, uint32_t img, uint32_t tile,
+                                           uint32_t old_state, WarpSmem& sm, uint32_t& parity, const Sched& sch) {
+  const CUtensorMap* tm_img = tmaps + 2 * img;
+  const CUtensorMap* tm_mask = tmaps + 2 * img + 1;
+  if (MODE == MODE_NS)
+    visit_ns(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+  else if (dd.ref_fma)
+    visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+  else
+    visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+}
+
+__device__ __forceinline__ WarpSmem& warp_slot(uint8_t* smem_raw) {
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  return reinterpret_cast<WarpSmem*>(base)[threadIdx.x >> 5];
+}
+
+__device__ __forceinline__ void warp_slot_init(WarpSmem& sm) {
+  if ((threadIdx.x & 31) == 0) {
+    mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+}
+
+// Image of a global tile id: binary search over the prefix array tile_base[0..n].
+__device__ __forceinline__ uint32_t image_of_tile(const uint32_t* tile_base, int n, uint32_t t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_base[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return (uint32_t)lo;
+}
+
+}  // namespace dtb

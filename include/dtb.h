@@ -1,0 +1,113 @@
+/*
+ * dtb.h -- C ABI of the B200 generalised geodesic distance transform (GGDT).
+ *
+ * This is the drop-in boundary for the reference library's GGDT entry points
+ * (namespace dt, dt/include/dt/generalised_distance_transform.hpp:7-27) and its transfer helpers
+ * (dt/include/dt/transfert.hpp:9-17).  Plain C: pointers, sizes and status codes; no C++ types, no
+ * exceptions, no torch types.  Every function is thread-safe per context; a context owns its device
+ * scratch and may be used from one thread at a time.
+ *
+ * Distances are FP32.  The map is the greatest fixpoint of single-edge relaxations from
+ * D = (mask != 0) ? 0 : v, i.e. the value the reference's raster rounds converge to
+ * (dt/src/generalised_distance_transform.cu:126-134), bit for bit.
+ */
+#ifndef DTB_H
+#define DTB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTB_API __attribute__((visibility("default")))
+#define DTB_ABI_VERSION 1
+
+typedef enum dtb_status {
+  DTB_OK = 0,
+  DTB_ERR_INVALID_ARG = 1,   /* bad size / kind / parameter (reference: assert in generalised_distance_transform.cu:104-107) */
+  DTB_ERR_CUDA = 2,          /* a CUDA runtime call failed (reference: std::runtime_error, generalised_distance_transform.cu:136-137) */
+  DTB_ERR_OUT_OF_MEMORY = 3, /* device allocation failed (reference: image2d_data_gpu.hpp:29-30) */
+  DTB_ERR_TIMEOUT = 4,       /* a bounded device wait gave up (no progress); the result is invalid */
+  DTB_ERR_DEVICE = 5,        /* the kernel reported an internal error (phase limit, ring full) */
+  DTB_ERR_NO_DEVICE = 6,     /* no usable sm_100 device */
+  DTB_ERR_CAPACITY = 7       /* a fixed-size limit was exceeded */
+} dtb_status;
+
+/* Memory kinds, reference dt::e_memory_kind (dt/include/dt/image2d_view.hpp:9-13). */
+typedef enum dtb_memory_kind { DTB_CPU = 0, DTB_GPU = 1 } dtb_memory_kind;
+
+/* A non-owning pitched 2-D view: the fields of dt::image2d_view<void> (image2d_view.hpp:117-123).
+ * Pixel (x, y) is at buffer + y * pitch + x * elem_size.
+ * elem_size: 1 = gray uint8 (or seed mask), 3 = rgb8 (interleaved r, g, b; reference dt::rgb8,
+ * dt/include/dt/rgb.hpp:7-12), 4 = float distances. */
+typedef struct dtb_image {
+  void* buffer;
+  int32_t width;
+  int32_t height;
+  int32_t pitch;       /* bytes between rows */
+  int32_t elem_size;   /* bytes per pixel */
+  int32_t memory_kind; /* dtb_memory_kind */
+} dtb_image;
+
+typedef struct dtb_context_s* dtb_context;
+
+/* Flags (bitwise or). */
+#define DTB_FLAG_ASYNC 0x1u       /* device images only: return after enqueueing; call dtb_sync() for the status */
+#define DTB_FLAG_ROUNDS 0x2u      /* plain per-image path: host-driven rounds over active tiles */
+#define DTB_FLAG_REF_NO_FMA 0x4u  /* ref-mode: round l_eucl*d and l_grad*|dI| separately instead of contracting */
+
+/* Counters of the last synchronous call (or of the call waited for by dtb_sync). */
+typedef struct dtb_stats {
+  uint64_t tiles;         /* tiles in the call */
+  uint64_t tile_visits;   /* warp visits of tiles (>= tiles reached) */
+  uint64_t phases;        /* sweep phases over all visits */
+  uint64_t activations;   /* neighbour re-activations issued */
+  uint64_t rounds;        /* host rounds (DTB_FLAG_ROUNDS), else 1 */
+  uint32_t device_error;  /* 0, or the device error code */
+  uint32_t device_error_info;
+} dtb_stats;
+
+DTB_API int32_t dtb_abi_version(void);
+DTB_API const char* dtb_status_string(dtb_status s);
+
+/* Context: owns device scratch (tile states, queue ring, descriptor tables, staging copies).
+ * device < 0 selects the current device. */
+DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out);
+DTB_API void dtb_context_destroy(dtb_context ctx);
+/* Detailed text of the last error of this context ("" if none). */
+DTB_API const char* dtb_context_message(dtb_context ctx);
+DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out);
+/* Waits for work enqueued with DTB_FLAG_ASYNC on `stream` and returns its device status. */
+DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
+
+/* Reference-weight GGDT (C8 neighbourhood, D(q) + (1-lambda)*{1, sqrt2} + lambda*|I(p)-I(q)|), gray input.
+ * Replaces dt::generalised_distance_transform (generalised_distance_transform.hpp:7-8),
+ * dt::generalised_distance_transform_blocks (:13-15) and dt::generalised_distance_transform_task (:21-23):
+ * all three converge to the same map.  img, mask: elem_size 1; dist: elem_size 4; same width/height.
+ * 0 <= lambda <= 1, v >= 0 (the reference default is v = 1e10).  Images may be CPU or GPU memory. */
+DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                               float lambda, float v, uint32_t flags, void* stream);
+
+/* Geodesic GGDT with C4 connectivity and w(p,q) = sqrt(1 + gamma^2 * |I(p)-I(q)|^2); gray (elem_size 1)
+ * or rgb8 (elem_size 3, |.| the Euclidean RGB difference).  Extends the reference entry point of
+ * generalised_distance_transform.hpp:7-8 to the C4 neighbourhood (dt/include/dt/c4.hpp:9-27) and rgb8. */
+DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                           float gamma, float v, uint32_t flags, void* stream);
+
+/* Ragged batch of n independent images (any mix of gray and rgb8, any sizes) in one persistent launch
+ * over a shared tile queue.  gammas[i] per image.  No reference counterpart (the reference runs one image
+ * per call). */
+DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
+                                 const dtb_image* dists, const float* gammas, float v, uint32_t flags, void* stream);
+
+/* Host <-> device copies of a pitched image, reference dt::host_to_device / dt::device_to_host
+ * (dt/include/dt/transfert.hpp:13-15, dt/src/transfert.cpp:10-28).  Synchronous when stream is NULL. */
+DTB_API dtb_status dtb_host_to_device(const dtb_image* src, const dtb_image* dst, void* stream);
+DTB_API dtb_status dtb_device_to_host(const dtb_image* src, const dtb_image* dst, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DTB_H */

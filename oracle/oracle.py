@@ -1,0 +1,118 @@
+"""ctypes front end of the CPU oracle (oracle/ggdt_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+reference legs, as the checker.  The product path (distance_transform_benchmarks_b200) never imports it.
+See ggdt_oracle.c for what is pinned against the reference (ref-mode: the two golden tensors of
+tests/distance_transform.cpp) and what is not (ns-mode: parity unpinned with respect to the reference).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build(force=False):
+    src = os.path.join(HERE, "ggdt_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(src) > os.path.getmtime(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []), check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, F, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
+        L.oracle_ggdt_ref.restype = I
+        L.oracle_ggdt_ref.argtypes = [P, I, P, I, P, I, I, F, F, I, I]
+        L.oracle_ggdt_ns.restype = I
+        L.oracle_ggdt_ns.argtypes = [P, I, I, P, I, P, I, I, F, F, I, I]
+        L.oracle_ggdt_ns_warm.restype = I
+        L.oracle_ggdt_ns_warm.argtypes = [P, I, I, P, I, P, I, I, F, I, I]
+        L.oracle_ggdt_ns_serial.restype = I
+        L.oracle_ggdt_ns_serial.argtypes = [P, I, I, P, I, P, I, I, F, F, I]
+        L.oracle_dijkstra_ns_f64.restype = I
+        L.oracle_dijkstra_ns_f64.argtypes = [P, I, I, P, I, P, I, I, D, D]
+        L.oracle_max_threads.restype = I
+        _lib = L
+    return _lib
+
+
+MAX_ROUNDS = 1 << 30
+
+
+def _c(a):
+    return np.ascontiguousarray(a)
+
+
+def g2_of(gamma):
+    """fl32(gamma * gamma), the squaring the CUDA path performs."""
+    g = np.float32(gamma)
+    return np.float32(g * g)
+
+
+def ggdt_ref(img, mask, lam, v=1e10, fma=True):
+    """ref-mode fixpoint (C8, lambda blend), gray uint8 [H, W]."""
+    img, mask = _c(img), _c(mask)
+    h, w = img.shape
+    d = np.empty((h, w), np.float32)
+    r = lib().oracle_ggdt_ref(img.ctypes.data, w, mask.ctypes.data, w, d.ctypes.data, w, h, float(lam), float(v),
+                              1 if fma else 0, MAX_ROUNDS)
+    if r < 0:
+        raise RuntimeError("oracle did not converge")
+    return d
+
+
+def ggdt_ns(img, mask, gamma, v=1e10, nthreads=0, serial=False):
+    """ns-mode fixpoint (C4, sqrt(1 + g2 dI^2)), gray [H, W] or rgb8 [H, W, 3]."""
+    img, mask = _c(img), _c(mask)
+    h, w = img.shape[:2]
+    ch = 3 if img.ndim == 3 else 1
+    d = np.empty((h, w), np.float32)
+    g2 = float(g2_of(gamma))
+    if serial:
+        r = lib().oracle_ggdt_ns_serial(img.ctypes.data, w * ch, ch, mask.ctypes.data, w, d.ctypes.data, w, h, g2,
+                                        float(v), MAX_ROUNDS)
+    else:
+        r = lib().oracle_ggdt_ns(img.ctypes.data, w * ch, ch, mask.ctypes.data, w, d.ctypes.data, w, h, g2, float(v),
+                                 int(nthreads), MAX_ROUNDS)
+    if r < 0:
+        raise RuntimeError("oracle did not converge")
+    return d
+
+
+def ggdt_ns_warm(img, new_seeds, prev, gamma, nthreads=0):
+    """Warm start from a previous ns-mode map with added seeds."""
+    img, new_seeds = _c(img), _c(new_seeds)
+    h, w = img.shape[:2]
+    ch = 3 if img.ndim == 3 else 1
+    d = np.array(prev, np.float32, copy=True, order="C")
+    r = lib().oracle_ggdt_ns_warm(img.ctypes.data, w * ch, ch, new_seeds.ctypes.data, w, d.ctypes.data, w, h,
+                                  float(g2_of(gamma)), int(nthreads), MAX_ROUNDS)
+    if r < 0:
+        raise RuntimeError("oracle did not converge")
+    return d
+
+
+def dijkstra_ns_f64(img, mask, gamma, v=1e10):
+    """Exact-sum FP64 Dijkstra on the ns-mode graph (weights evaluated in double from g2 = fl32(gamma^2))."""
+    img, mask = _c(img), _c(mask)
+    h, w = img.shape[:2]
+    ch = 3 if img.ndim == 3 else 1
+    d = np.empty((h, w), np.float64)
+    r = lib().oracle_dijkstra_ns_f64(img.ctypes.data, w * ch, ch, mask.ctypes.data, w, d.ctypes.data, w, h,
+                                     float(g2_of(gamma)), float(v))
+    if r != 0:
+        raise MemoryError("dijkstra allocation failed")
+    return d
+
+
+def max_threads():
+    return lib().oracle_max_threads()

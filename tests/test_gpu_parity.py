@@ -1,0 +1,224 @@
+"""GPU parity tests: the CUDA path against the oracle, bit for bit.
+
+Mirrors the reference's tests/distance_transform.cpp: the two golden tensors (:14-281, :283-476) through all
+three entry points, and cross-variant equality on random images (:485-559) -- here seeded, and against the
+oracle rather than against another GPU variant.  Full-size workloads are checked through the exact fixpoint
+characterisation of tests/helpers.py.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import distance_transform_benchmarks_b200 as dtb
+from distance_transform_benchmarks_b200 import workloads as wl
+from oracle import oracle as orc
+from tests.helpers import assert_images_eq, ns_fixpoint_violations
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_goldens.npz"))
+VARIANTS = {
+    "raster": dtb.generalised_distance_transform,
+    "blocks": dtb.generalised_distance_transform_blocks,
+    "task": dtb.generalised_distance_transform_task,
+}
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+# ---------------------------------------------------------------------------------------------------
+# ref-mode (reference weight, C8)
+# ---------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+@pytest.mark.parametrize("name", ["euclid", "geodesic"])
+def test_reference_goldens(ctx, variant, name):
+    img, mask, ref = GOLD[name + "_img"], GOLD[name + "_mask"], GOLD[name + "_ref"]
+    d = VARIANTS[variant](cuda(img), cuda(mask), float(GOLD[name + "_lambda"]), ctx=ctx)
+    assert_images_eq(d, ref, "%s %s" % (variant, name))
+
+
+REF_SIZES = [(1, 1), (1, 37), (37, 1), (31, 33), (32, 32), (64, 64), (100, 300), (230, 250)]
+
+
+def _ref_case(h, w, seed):
+    rng = np.random.default_rng(seed)
+    img = rng.integers(0, 256, (h, w), dtype=np.uint8)
+    mask = np.zeros((h, w), np.uint8)
+    mask[h // 2, w // 2] = 1
+    for _ in range(2):
+        mask[rng.integers(0, h), rng.integers(0, w)] = 1
+    return img, mask
+
+
+@pytest.mark.parametrize("h,w", REF_SIZES)
+@pytest.mark.parametrize("lam", [0.0, 0.5, 1.0, 0.3])
+def test_ref_random_vs_oracle(ctx, h, w, lam):
+    img, mask = _ref_case(h, w, h * 1000 + w)
+    ref = orc.ggdt_ref(img, mask, lam, fma=True)
+    for variant in ("task", "blocks"):
+        d = VARIANTS[variant](cuda(img), cuda(mask), lam, ctx=ctx)
+        assert_images_eq(d, ref, "ref %s %dx%d lambda=%g" % (variant, w, h, lam))
+
+
+@pytest.mark.parametrize("lam", [0.3, 0.77])
+def test_ref_no_fma_vs_oracle(ctx, lam):
+    img, mask = _ref_case(90, 70, 5)
+    ref = orc.ggdt_ref(img, mask, lam, fma=False)
+    d = dtb.generalised_distance_transform(cuda(img), cuda(mask), lam, ctx=ctx, fma=False)
+    assert_images_eq(d, ref, "ref no-fma lambda=%g" % lam)
+
+
+def test_ref_smooth_image_multi_seed(ctx):
+    img = wl.blobs_gray(17, 200, 150)
+    mask = wl.random_disks(np.random.default_rng(4), 200, 150, 6, 1, 4)
+    ref = orc.ggdt_ref(img, mask, 0.5)
+    assert_images_eq(dtb.generalised_distance_transform(cuda(img), cuda(mask), 0.5, ctx=ctx), ref, "ref blobs")
+
+
+# ---------------------------------------------------------------------------------------------------
+# ns-mode (C4, sqrt(1 + gamma^2 dI^2))
+# ---------------------------------------------------------------------------------------------------
+def _ns_check(ctx, img, mask, gamma, v=1e10, what="", rounds=(False, True)):
+    ref = orc.ggdt_ns(img, mask, gamma, v=v)
+    for r in rounds:
+        d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, v=v, rounds=r, ctx=ctx)
+        assert_images_eq(d, ref, "%s rounds=%s" % (what, r))
+    return ref
+
+
+def test_ns_config0(ctx):
+    img, mask, gamma = wl.config0()
+    _ns_check(ctx, img, mask, gamma, what="config0")
+
+
+@pytest.mark.parametrize("h,w", [(1, 1), (1, 50), (50, 1), (33, 65), (129, 97), (256, 256)])
+@pytest.mark.parametrize("rgb", [False, True])
+def test_ns_odd_sizes_random(ctx, h, w, rgb):
+    rng = np.random.default_rng(h * 7 + w)
+    img = rng.integers(0, 256, (h, w, 3) if rgb else (h, w), dtype=np.uint8)
+    mask = np.zeros((h, w), np.uint8)
+    mask[rng.integers(0, h), rng.integers(0, w)] = 1
+    _ns_check(ctx, img, mask, 0.2, what="random %dx%d rgb=%s" % (w, h, rgb))
+
+
+def test_ns_voronoi_rgb(ctx):
+    img = wl.voronoi_rgb(21, 333, 250)
+    mask = wl.random_disks(np.random.default_rng(9), 333, 250, 8, 5, 5)
+    _ns_check(ctx, img, mask, 0.02, what="voronoi")
+
+
+def test_ns_maze_crop(ctx):
+    img, (sx, sy) = wl.maze_gray(31, 512, 512)
+    mask = np.zeros(img.shape, np.uint8)
+    mask[sy, sx] = 1
+    _ns_check(ctx, img, mask, 0.5, what="maze 512")
+
+
+def test_ns_no_seeds_all_v(ctx):
+    img = wl.blobs_gray(3, 100, 70)
+    mask = np.zeros(img.shape, np.uint8)
+    d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), 0.1, v=55.0, ctx=ctx)
+    assert bool((d == 55.0).all())
+
+
+def test_ns_all_seeds_zero(ctx):
+    img = wl.blobs_gray(3, 70, 100)
+    mask = np.ones(img.shape, np.uint8)
+    d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), 0.1, ctx=ctx)
+    assert bool((d == 0).all())
+
+
+def test_ns_corner_seeds_and_inf_v(ctx):
+    img = wl.blobs_gray(8, 97, 131)
+    mask = np.zeros(img.shape, np.uint8)
+    mask[0, 0] = mask[-1, -1] = 1
+    _ns_check(ctx, img, mask, 1.0, v=float("inf"), what="corners inf-v")
+
+
+def test_ns_unaligned_pitch_is_staged(ctx):
+    img = wl.blobs_gray(12, 37, 29)  # 37-byte rows: not TMA-aligned, staged by the library
+    mask = np.zeros(img.shape, np.uint8)
+    mask[3, 4] = 1
+    _ns_check(ctx, img, mask, 0.3, what="unaligned", rounds=(False,))
+
+
+def test_ns_padded_views(ctx):
+    big = cuda(wl.blobs_gray(13, 160, 90))
+    img = big[:, 16:144]  # pitch 160, offset 16 bytes: aligned sub-view
+    mask = torch.zeros((90, 128), dtype=torch.uint8, device="cuda")
+    mask[40, 60] = 1
+    dist_big = torch.full((90, 200), -1.0, device="cuda")
+    dist = dist_big[:, 8:136]
+    dtb.geodesic_distance_transform(img, mask, 0.1, dist=dist, ctx=ctx)
+    ref = orc.ggdt_ns(img.cpu().numpy(), mask.cpu().numpy(), 0.1)
+    assert_images_eq(dist, ref, "padded view")
+    assert bool((dist_big[:, :8] == -1).all()) and bool((dist_big[:, 136:] == -1).all())
+
+
+def test_ns_host_buffers(ctx):
+    img, mask, gamma = wl.config0(seed=5, w=300, h=200)
+    dist = torch.empty((200, 300), dtype=torch.float32)
+    dtb.geodesic_distance_transform(torch.from_numpy(img), torch.from_numpy(mask), gamma, dist=dist, ctx=ctx)
+    assert_images_eq(dist, orc.ggdt_ns(img, mask, gamma), "host buffers")
+
+
+def test_ns_repeated_calls_are_identical(ctx):
+    img, mask, gamma = wl.config0(seed=6)
+    a = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=ctx)
+    for _ in range(3):
+        b = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=ctx)
+        assert_images_eq(b, a.cpu().numpy(), "repeat")
+
+
+def test_ns_fp64_relative_error_config0(ctx):
+    img, mask, gamma = wl.config0()
+    d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=ctx).cpu().numpy()
+    dj = orc.dijkstra_ns_f64(img, mask, gamma)
+    assert float((np.abs(d - dj) / np.maximum(dj, 1e-30)).max()) < 1e-5
+
+
+# ---------------------------------------------------------------------------------------------------
+# ragged batch
+# ---------------------------------------------------------------------------------------------------
+def test_batch_vs_oracle_and_single(ctx):
+    batch = wl.config3(seed=11, n=24, smin=16, smax=300)
+    imgs = [cuda(i) for i, _, _ in batch]
+    masks = [cuda(m) for _, m, _ in batch]
+    gammas = [g for _, _, g in batch]
+    dists = dtb.geodesic_distance_transform_batch(imgs, masks, gammas, ctx=ctx)
+    for k, ((img, mask, g), d) in enumerate(zip(batch, dists)):
+        assert_images_eq(d, orc.ggdt_ns(img, mask, g), "batch image %d %s" % (k, img.shape))
+    st = ctx.stats()
+    assert st["tiles"] == sum(((i.shape[0] + 31) // 32) * ((i.shape[1] + 31) // 32) for i, _, _ in batch)
+    assert st["tile_visits"] >= 1 and st["device_error"] == 0
+    plain = dtb.geodesic_distance_transform_batch(imgs, masks, gammas, rounds=True, ctx=ctx)
+    for k, (a, b) in enumerate(zip(dists, plain)):
+        assert_images_eq(b, a.cpu().numpy(), "plain per-image vs batch %d" % k)
+
+
+def test_batch_host_buffers(ctx):
+    batch = wl.config3(seed=12, n=6, smin=40, smax=200)
+    dists = dtb.geodesic_distance_transform_batch([torch.from_numpy(i) for i, _, _ in batch],
+                                                  [torch.from_numpy(m) for _, m, _ in batch],
+                                                  [g for _, _, g in batch], ctx=ctx)
+    for (img, mask, g), d in zip(batch, dists):
+        assert not d.is_cuda
+        assert_images_eq(d, orc.ggdt_ns(img, mask, g), "batch host")
+
+
+# ---------------------------------------------------------------------------------------------------
+# full-size configurations: exact fixpoint characterisation (size independent)
+# ---------------------------------------------------------------------------------------------------
+@pytest.mark.parametrize("which", ["config1", "config2"])
+def test_full_size_fixpoint(ctx, which):
+    img, mask, gamma = getattr(wl, which)()
+    ti, tm = cuda(img), cuda(mask)
+    d = dtb.geodesic_distance_transform(ti, tm, gamma, ctx=ctx)
+    va, vb, dmax = ns_fixpoint_violations(ti, tm, gamma, 1e10, d)
+    assert dmax < 2 ** 23, dmax
+    assert va == 0 and vb == 0, (va, vb)
+    assert ctx.stats()["device_error"] == 0
