@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark: converged GGDT Mpixel/s on the ragged batch (1024 images, sides log-uniform in [64, 2048],
+half gray blobs / half rgb8 Voronoi, 1-8 seed disks, gamma in {0.01, 0.1, 1.0}), one persistent launch per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Under torchrun every rank processes its own batch (different seed, no data-path
+collective: images are independent), so per-GPU work is fixed (weak scaling); the step time is the max over
+ranks.  `value` times the batch on device-resident inputs; `e2e` times the same call through the C ABI with
+pinned host buffers (host->device copies of images and masks and the device->host copy of the distance
+maps inside the timed region).  `--impl reference` times the CPU restatement of the reference algorithm
+(the reference has no CPU implementation of this path) on the host cores.
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged GGDT Mpixel/s, batched vs per-image on one B200; serve p50/p99 ms"
+UNIT = "Mpixel/s"
+PLAIN_SUBSET = 64          # images of the batch timed through the plain per-image path
+CPU_SAMPLE_SECONDS = 15.0  # bounded CPU baseline sample
+REF_STEP_MPX = 24.0        # reference arm: pixels per step
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--images", type=int, default=1024)
+    p.add_argument("--seed", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------------------
+# distributed plumbing (timing only: the max of the step times over ranks)
+# ---------------------------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+
+    def init(self, backend):
+        if self.world > 1:
+            import torch.distributed as td
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as td
+            td.barrier()
+
+    def max(self, x, device):
+        if not self.pg:
+            return x
+        import torch.distributed as td
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x, device):
+        if not self.pg:
+            return x
+        import torch.distributed as td
+        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+        td.all_reduce(t, op=td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as td
+            td.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        self.path = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(device).uuid)
+            self.sel = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            self.sel = str(device)
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.sel, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "50", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.15)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_bytes_per_px():
+    """DRAM bytes per pixel of the tile kernel from the committed ncu summary (a smaller capture of the same
+    workload, scaled by pixels), or None."""
+    path = os.path.join(ROOT, "profiles", "ggdt_persistent_batch.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_pixel:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------------------------------------
+def cpu_baseline(batch, seconds):
+    """The oracle (CPU restatement of the reference raster algorithm) on the host cores, over the batch's
+    images in order until `seconds` of work: Mpixel/s."""
+    from oracle import oracle as orc
+    px, t0 = 0, time.perf_counter()
+    n = 0
+    for img, mask, g in batch:
+        orc.ggdt_ns(img, mask, g)
+        px += img.shape[0] * img.shape[1]
+        n += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": px / dt / 1e6, "unit": UNIT, "cores": orc.max_threads(), "kind": "port",
+            "sample": "first %d images of the batch (%.1f Mpx), %.1f s" % (n, px / 1e6, dt)}
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    from distance_transform_benchmarks_b200 import workloads as wl
+    from oracle import oracle as orc
+    specs = wl.config3_specs(seed=args.seed, n=args.images)
+    sample, px = [], 0
+    for s in specs:
+        sample.append(wl.make_image(s))
+        px += s[1] * s[2]
+        if px >= REF_STEP_MPX * 1e6:
+            break
+    for _ in range(args.warmup):
+        for img, mask, g in sample[:4]:
+            orc.ggdt_ns(img, mask, g)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for img, mask, g in sample:
+            orc.ggdt_ns(img, mask, g)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = px / 1e6 / (ms / 1e3)
+    desc = "first %d images of the 1024-image batch (%.1f Mpx) per step" % (len(sample), px / 1e6)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ragged batch of 1024 images (sides log-U[64,2048], gray blobs / rgb8 Voronoi)",
+                       "sample": desc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": orc.max_threads(), "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, dist):
+    import distance_transform_benchmarks_b200 as dtb
+    from distance_transform_benchmarks_b200 import workloads as wl
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    ctx = dtb.Context(dev)
+    stream = torch.cuda.current_stream()
+
+    batch = wl.config3(seed=args.seed + 1000 * dist.rank, n=args.images)
+    px = wl.pixels(batch)
+    alg_bytes = sum(img.shape[0] * img.shape[1] * wl.bytes_per_pixel(img) for img, _, _ in batch)
+    imgs = [torch.from_numpy(i).cuda() for i, _, _ in batch]
+    masks = [torch.from_numpy(m).cuda() for _, m, _ in batch]
+    gammas = [g for _, _, g in batch]
+    dists = [torch.empty(i.shape[:2], dtype=torch.float32, device="cuda") for i, _, _ in batch]
+
+    def step(timing=False):
+        dtb.geodesic_distance_transform_batch(imgs, masks, gammas, dists=dists, ctx=ctx, stream=stream, timing=timing)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    stats = ctx.stats()
+
+    clocks = Clocks(dev)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kernel_ms = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(timing=True)
+        kernel_ms.append(ctx.stats()["kernel_ms"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_max = dist.max(ms, "cuda")
+    px_all = dist.sum(px, "cuda")
+    value = px_all / 1e6 / (ms_max / 1e3)
+
+    # Plain per-image path (host-driven rounds, one image per call) and persistent per-image calls.
+    sub = slice(0, min(PLAIN_SUBSET, len(batch)))
+    px_sub = sum(i.shape[0] * i.shape[1] for i, _, _ in batch[sub])
+    for _ in range(2):
+        dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx,
+                                              stream=stream, rounds=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx, stream=stream,
+                                          rounds=True)
+    torch.cuda.synchronize()
+    plain = px_sub / 1e6 / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for k in range(sub.stop):
+        dtb.geodesic_distance_transform(imgs[k], masks[k], gammas[k], dist=dists[k], ctx=ctx, stream=stream)
+    torch.cuda.synchronize()
+    per_image_persistent = px_sub / 1e6 / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx, stream=stream)
+    torch.cuda.synchronize()
+    batched_sub = px_sub / 1e6 / (time.perf_counter() - t0)
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        himgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
+        hmasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]
+        hdists = [torch.empty(i.shape[:2], dtype=torch.float32).pin_memory() for i, _, _ in batch]
+        h2d = sum(t.numel() * t.element_size() for t in himgs + hmasks)
+        d2h = sum(t.numel() * t.element_size() for t in hdists)
+
+        def estep():
+            dtb.geodesic_distance_transform_batch(himgs, hmasks, gammas, dists=hdists, ctx=ctx, stream=stream)
+
+        for _ in range(2):
+            estep()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            estep()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = dist.max(e0.elapsed_time(e1) / args.steps, "cuda")
+        e2e = {"value": px_all / 1e6 / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": ems}
+        ok = all(torch.equal(hd, d.cpu()) for hd, d in zip(hdists[:8], dists[:8]))
+        e2e["matches_device_run"] = bool(ok)
+
+    kms = statistics.mean(kernel_ms) if kernel_ms and kernel_ms[0] > 0 else None
+    peak, peak_kind = measured_peak_gbs()
+    roofline = None
+    if kms:
+        achieved = alg_bytes / (kms / 1e3) / 1e9
+        bpp = profiled_traffic_bytes_per_px()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_kind": peak_kind, "kernel": "ggdt_persistent", "kernel_ms": kms,
+                    "algorithmic_bytes": alg_bytes, "traffic": (bpp * px) if bpp else None}
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(batch, CPU_SAMPLE_SECONDS)
+
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "ragged batch of %d images per GPU, sides log-U[64,2048], half gray blobs / half "
+                                       "rgb8 Voronoi, 1-8 seed disks r 2-6, gamma in {0.01,0.1,1.0}" % args.images,
+                           "pixels_per_gpu": px, "parallelism": "replicas (independent images per rank)",
+                           "l2": "inputs larger than L2 (no flush needed)", "launch": "one persistent launch per step"},
+                "per_image": {"plain_rounds_mpx_s": plain, "persistent_per_image_mpx_s": per_image_persistent,
+                              "batched_same_subset_mpx_s": batched_sub, "subset_images": sub.stop,
+                              "batched_vs_plain": value / plain if plain else None},
+                "tile_stats": {"tiles": stats["tiles"], "visits_per_tile": stats["tile_visits"] / max(1, stats["tiles"]),
+                               "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},
+                "gpu_launches": 3 * args.steps,
+                "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        run_reference(args, dist)  # rank 0 only; the other ranks exit without work
+        return
+    dist.init("nccl")
+    try:
+        run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -15,8 +15,8 @@ import threading
 import numpy as np
 import torch
 
-from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_GPU, DtbError, DtbImage,
-                      DtbStats, lib)
+from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_FLAG_TIMING, DTB_GPU, DtbError,
+                      DtbImage, DtbStats, lib)
 
 __all__ = [
     "Context", "DtbError", "default_context", "generalised_distance_transform",
@@ -177,7 +177,7 @@ def geodesic_distance_transform(img, mask, gamma, v=DEFAULT_V, dist=None, *, rou
 
 
 def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=None, *, rounds=False, ctx=None,
-                                      stream=None, asynchronous=False):
+                                      stream=None, asynchronous=False, timing=False):
     """Ragged batch in one persistent launch over a shared tile queue (dtb_gdt_batch)."""
     n = len(imgs)
     imgs = [_as_tensor(t) for t in imgs]
@@ -193,7 +193,8 @@ def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=No
     vm = (DtbImage * n)(*[image_view(t, 1) for t in masks])
     vd = (DtbImage * n)(*[image_view(t, 4) for t in dists])
     g = (ctypes.c_float * n)(*[float(x) for x in gammas])
-    flags = (DTB_FLAG_ROUNDS if rounds else 0) | (DTB_FLAG_ASYNC if asynchronous else 0)
+    flags = (DTB_FLAG_ROUNDS if rounds else 0) | (DTB_FLAG_ASYNC if asynchronous else 0) | \
+        (DTB_FLAG_TIMING if timing else 0)
     ctx.check(lib().dtb_gdt_batch(ctx.handle, n, vi, vm, vd, g, float(v), flags, ctypes.c_void_p(_stream_ptr(stream))))
     return dists
 

@@ -15,6 +15,7 @@ DTB_GPU = 1
 DTB_FLAG_ASYNC = 0x1
 DTB_FLAG_ROUNDS = 0x2
 DTB_FLAG_REF_NO_FMA = 0x4
+DTB_FLAG_TIMING = 0x8
 
 STATUS_NAMES = {
     0: "DTB_OK", 1: "DTB_ERR_INVALID_ARG", 2: "DTB_ERR_CUDA", 3: "DTB_ERR_OUT_OF_MEMORY", 4: "DTB_ERR_TIMEOUT",
@@ -50,6 +51,7 @@ class DtbStats(ctypes.Structure):
         ("rounds", ctypes.c_uint64),
         ("device_error", ctypes.c_uint32),
         ("device_error_info", ctypes.c_uint32),
+        ("kernel_ms", ctypes.c_double),
     ]
 
 

@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
   uint32_t parity = 0;
   const QueueSched sch{q, states};
   const int lane = threadIdx.x & 31;
+  WarpStats ws;
   for (;;) {
     uint32_t t = POP_NONE, old = 0;
     if (lane == 0) {
@@ -89,8 +90,9 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     old = __shfl_sync(~0u, old, 0);
     const uint32_t img = old >> ST_IMG_SHIFT;
     const ImgDesc dd = descs[img];
-    visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch);
+    visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws);
   }
+  flush_stats(ws, q);
 }
 
 // One host-driven round: one warp per tile, inactive tiles return at once.
@@ -108,7 +110,9 @@ __global__ void __launch_bounds__(WPC * 32)
   const uint32_t img = old >> ST_IMG_SHIFT;
   const RoundSched sch{q, states, next_active, changed};
   const ImgDesc dd = descs[img];
-  visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch);
+  WarpStats ws;
+  visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws);
+  flush_stats(ws, q);
 }
 
 // Tiles never reached keep uninitialised memory: write v there.
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__
 namespace {
 
 constexpr int PERSIST_WPC = 4;
-constexpr int PERSIST_MINB = 4;
+constexpr int PERSIST_MINB = 2;
 constexpr int ROUND_WPC = 4;
 constexpr size_t SMEM_SLOT = sizeof(WarpSmem);
 constexpr size_t PERSIST_SMEM = PERSIST_WPC * SMEM_SLOT + 128;
@@ -170,6 +174,8 @@ struct dtb_context_s {
   QueueHdr* last_hdr = nullptr;
   uint64_t last_tiles = 0;
   cudaStream_t last_stream = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
+  bool timed = false;
   bool async_pending = false;
   std::mutex mu;
 };
@@ -407,10 +413,12 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
       attr[0].val.cooperative = 1;
       cfg.attrs = attr;
       cfg.numAttrs = 1;
+      if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], stream));
       if (mode == MODE_NS)
         DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
       else
         DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
+      if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], stream));
     } else {
       DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
       ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, act0, 0);
@@ -460,6 +468,7 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   ctx->last_tiles = total;
   ctx->last_stream = stream;
   ctx->stats = dtb_stats{};
+  ctx->timed = (flags & DTB_FLAG_TIMING) && !rounds && total > 0;
   ctx->stats.tiles = total;
   ctx->stats.rounds = nrounds;
   const bool async = (flags & DTB_FLAG_ASYNC) && !host_out && !host_in;
@@ -515,6 +524,10 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
     return DTB_ERR_NO_DEVICE;
   }
   ctx->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess) {
+    delete ctx;
+    return DTB_ERR_NO_DEVICE;
+  }
   const void* kp[2] = {(const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>,
                         (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>};
   const void* kr[2] = {(const void*)ggdt_round<MODE_NS, ROUND_WPC>, (const void*)ggdt_round<MODE_REF, ROUND_WPC>};
@@ -537,6 +550,8 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
   if (ctx->dscratch) cudaFree(ctx->dscratch);
   if (ctx->dstage) cudaFree(ctx->dstage);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
   delete ctx;
 }
 
@@ -561,6 +576,12 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream) {
   ctx->stats.activations = h.activations.v;
   ctx->stats.device_error = h.error.v;
   ctx->stats.device_error_info = h.err_info.v;
+  if (ctx->timed) {
+    float ms = 0.0f;
+    DTB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->stats.kernel_ms = ms;
+    ctx->timed = false;
+  }
   switch (h.error.v) {
     case DERR_NONE: return DTB_OK;
     case DERR_QUEUE_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "tile queue made no progress within the time limit (ticket %u)", h.err_info.v);

@@ -66,10 +66,11 @@ struct QueueHdr {
   Line tail;       // next push position
   Line pending;    // tiles queued or running
   Line error;      // first device error code
-  Line progress;   // completed visits (used by the no-progress watchdog)
+  Line progress;   // completed visits (flushed per warp in batches; watchdog and visit cap)
   Line phases;     // total sweep phases
   Line activations;  // neighbour activations issued
   Line err_info;   // tile id / detail of the first error
+  Line done;       // set once when pending reached 0
 };
 
 struct Queue {
@@ -137,60 +138,88 @@ __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
 
 // ------------------------------------------------------------------------------------------------------
 // Queue: a ticket ring of tile ids with a pending counter for termination.
-//   push: pending += 1, then a tail ticket, then the item into its slot (slot must be free: CAS from 0).
-//   pop:  a head ticket, then wait until its slot holds an item, or until pending == 0 (done), or error.
+//   push: pending grows first, then a tail range is reserved, then each item goes into its slot (the slot
+//         must be free: CAS from 0).
+//   pop:  a head ticket, then the popper waits on its own slot only (no shared hot line is polled), until
+//         an item or the termination sentinel arrives.  Termination: the visit whose completion brings
+//         pending to 0 sets `done` and writes the sentinel into every slot that has a waiting popper.
 // Items are interchangeable, so a popper that takes an item meant for another ticket of the same slot is
-// harmless: every item is taken exactly once (atomicExch) and no slot is written twice (CAS from 0).
+// harmless: every item is taken exactly once (atomicExch) and no slot is written twice (CAS from 0).  The
+// ring holds at least 2 * (tiles + workers) slots, more than items and waiting poppers together.
 // All waits are bounded by a no-global-progress watchdog and end with an error code, never a hang.
 // ------------------------------------------------------------------------------------------------------
+constexpr uint32_t SLOT_SENTINEL = 0xFFFFFFFFu;  // never an item: items are tile id + 1 < 2^31
+constexpr uint32_t POP_NONE = 0xFFFFFFFFu;
+constexpr uint64_t POLL_CHECK_NS = 20000;        // rare checks of done / error / watchdog while waiting
+
 __device__ __forceinline__ void set_error(const Queue& q, uint32_t code, uint32_t info) {
   if (atomicCAS(&q.hdr->error.v, 0u, code) == 0u) atomicExch(&q.hdr->err_info.v, info);
 }
 
-__device__ __forceinline__ void queue_push(const Queue& q, uint32_t item) {
-  atomicAdd(&q.hdr->pending.v, 1u);
-  const uint32_t p = atomicAdd(&q.hdr->tail.v, 1u);
+// Writes item into ring position p once the slot is free (bounded wait).
+__device__ __forceinline__ void slot_write(const Queue& q, uint32_t p, uint32_t item) {
   uint32_t* slot = &q.ring[p & q.mask];
+  if (atomicCAS(slot, 0u, item + 1u) == 0u) return;
   uint32_t ns = 32;
   const uint64_t t0 = globaltimer();
   while (atomicCAS(slot, 0u, item + 1u) != 0u) {
-    if (globaltimer() - t0 > q.timeout_ns) { set_error(q, DERR_RING_FULL, item); atomicSub(&q.hdr->pending.v, 1u); return; }
+    if (globaltimer() - t0 > q.timeout_ns) { set_error(q, DERR_RING_FULL, item); return; }
     __nanosleep(ns);
     ns = ns < 1024 ? ns * 2 : ns;
   }
 }
 
-constexpr uint32_t POP_NONE = 0xFFFFFFFFu;
+// Single-item push (seed scan): pending += 1 before the item becomes visible.
+__device__ __forceinline__ void queue_push(const Queue& q, uint32_t item) {
+  atomicAdd(&q.hdr->pending.v, 1u);
+  __threadfence();
+  slot_write(q, atomicAdd(&q.hdr->tail.v, 1u), item);
+}
+
+// Called by the whole warp of the visit that brought pending to 0.
+__device__ __forceinline__ void signal_done_warp(const Queue& q) {
+  const int lane = threadIdx.x & 31;
+  uint32_t h = 0, t = 0;
+  if (lane == 0) {
+    atomicExch(&q.hdr->done.v, 1u);
+    __threadfence();
+    h = ld_volatile(&q.hdr->head.v);
+    t = ld_volatile(&q.hdr->tail.v);
+  }
+  h = __shfl_sync(~0u, h, 0);
+  t = __shfl_sync(~0u, t, 0);
+  for (uint32_t p = t + (uint32_t)lane; (int32_t)(h - p) > 0; p += 32u)
+    *(volatile uint32_t*)&q.ring[p & q.mask] = SLOT_SENTINEL;
+}
 
 // Called by one lane.  Returns a tile id or POP_NONE (queue drained, or error).
 __device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
   const uint32_t h = atomicAdd(&q.hdr->head.v, 1u);
+  __threadfence();  // the ticket before the checks below (pairs with the fence of signal_done_warp)
+  if (ld_volatile(&q.hdr->done.v) | ld_volatile(&q.hdr->error.v)) return POP_NONE;
+  if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;  // nothing queued at all
   uint32_t* slot = &q.ring[h & q.mask];
-  uint32_t ns = 16;
-  uint64_t t0 = 0;
-  uint32_t seen = 0;
-  for (uint32_t it = 0;; ++it) {
+  uint32_t ns = 32;
+  uint64_t t_check = globaltimer(), t_prog = t_check;
+  uint32_t seen = ld_volatile(&q.hdr->progress.v);
+  for (;;) {
     if (ld_volatile(slot) != 0u) {
       const uint32_t v = atomicExch(slot, 0u);
-      if (v != 0u) {
-        if (ld_volatile(&q.hdr->progress.v) > q.max_visits) {
-          set_error(q, DERR_VISIT_LIMIT, v - 1u);
-          return POP_NONE;  // the item is dropped: the call has failed anyway
-        }
-        return v - 1u;
-      }
-    }
-    if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;
-    if (ld_volatile(&q.hdr->error.v) != 0u) return POP_NONE;
-    if ((it & 15u) == 0u) {
-      const uint32_t prog = ld_volatile(&q.hdr->progress.v);
-      if (prog > q.max_visits) { set_error(q, DERR_VISIT_LIMIT, prog); return POP_NONE; }
-      const uint64_t now = globaltimer();
-      if (it == 0 || prog != seen) { seen = prog; t0 = now; }
-      else if (now - t0 > q.timeout_ns) { set_error(q, DERR_QUEUE_TIMEOUT, h); return POP_NONE; }
+      if (v == SLOT_SENTINEL) return POP_NONE;
+      if (v != 0u) return v - 1u;
     }
     __nanosleep(ns);
-    ns = ns < 512 ? ns * 2 : ns;
+    ns = ns < 256 ? ns * 2 : ns;
+    const uint64_t now = globaltimer();
+    if (now - t_check > POLL_CHECK_NS) {
+      t_check = now;
+      if (ld_volatile(&q.hdr->done.v) | ld_volatile(&q.hdr->error.v)) return POP_NONE;
+      if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;
+      const uint32_t prog = ld_volatile(&q.hdr->progress.v);
+      if (prog > q.max_visits) { set_error(q, DERR_VISIT_LIMIT, prog); return POP_NONE; }
+      if (prog != seen) { seen = prog; t_prog = now; }
+      else if (now - t_prog > q.timeout_ns) { set_error(q, DERR_QUEUE_TIMEOUT, h); return POP_NONE; }
+    }
   }
 }
 
@@ -215,26 +244,45 @@ __device__ __forceinline__ float ref_relax(float dq, float eucl_d, float l_eucl,
 }
 
 // ------------------------------------------------------------------------------------------------------
-// One phase along a line of 32 pixels held in registers: a forward chain from `lo` (the halo before
-// d[0]) and a backward chain from `hi` (the halo after d[31]), interleaved for two independent dependency
-// chains.  w[k] is the weight of the edge between positions k-1 and k (w[0]: lo -> d[0], w[32]: d[31] ->
-// hi).  Each step is one single-edge relaxation fl(D + w); after the phase every edge of the line is
-// satisfied in both directions.  Returns whether any value decreased.
+// One phase of the warp's tile in either layout.  Lane l holds a line of 32 pixels d[0..31] (a row in the
+// row layout, a column in the column layout); lanes l-1 / l+1 hold the neighbouring lines.
+//   chain edges  wc[k]: between positions k-1 and k of the own line (wc[0]: lo -> d[0], wc[32]: d[31] -> hi,
+//                where lo / hi are the halo pixels before and after the line);
+//   cross edges  wx[k]: between position k of line l-1 and position k of line l.
+// A forward chain walks k = 0..31 and a backward chain k = 31..0, interleaved (two independent dependency
+// chains).  At each step the chain pixel is first relaxed along the line (from its predecessor on the
+// chain), then across the lines from both neighbouring lanes, whose values at the same position are
+// exchanged by warp shuffles.  Every step is a set of single-edge relaxations fl(D + w): no two edge weights
+// are ever added before meeting a distance, so the result is the exact fixpoint whatever the order.  A chain
+// therefore follows any staircase path that moves at most one line per position, in both cross directions,
+// so one phase covers every monotone path of slope <= 1 along its axis.  Every internal edge of the tile is
+// relaxed in both directions during a phase: a phase that changes nothing proves the tile internally
+// converged.  The halo lines of the cross direction are not read here (lane 0 / 31 shuffle with themselves,
+// which never lowers a value); they are the chain halo of the other layout's phase.
 // ------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ bool sweep_line(float (&d)[TILE], const float (&w)[TILE + 1], float lo, float hi) {
+__device__ __forceinline__ bool sweep_phase(float (&d)[TILE], const float (&wc)[TILE + 1], const float (&wx)[TILE], float lo,
+                                            float hi) {
   bool ch = false;
   float f = lo, b = hi;
 #pragma unroll
   for (int k = 0; k < TILE; ++k) {
-    const int yf = k, yb = TILE - 1 - k;
-    const float t = __fadd_rn(f, w[yf]);
-    ch |= t < d[yf];
-    d[yf] = fminf(d[yf], t);
-    f = d[yf];
-    const float u = __fadd_rn(b, w[yb + 1]);
-    ch |= u < d[yb];
-    d[yb] = fminf(d[yb], u);
-    b = d[yb];
+    const int i = k, j = TILE - 1 - k;
+    const float di = d[i];
+    const float a = fminf(di, __fadd_rn(f, wc[i]));
+    const float from_prev = __shfl_up_sync(~0u, a, 1);
+    const float from_next = __shfl_down_sync(~0u, __fadd_rn(a, wx[i]), 1);
+    const float c = fminf(a, fminf(__fadd_rn(from_prev, wx[i]), from_next));
+    ch |= c < di;
+    d[i] = c;
+    f = c;
+    const float dj = d[j];
+    const float e = fminf(dj, __fadd_rn(b, wc[j + 1]));
+    const float from_prev2 = __shfl_up_sync(~0u, e, 1);
+    const float from_next2 = __shfl_down_sync(~0u, __fadd_rn(e, wx[j]), 1);
+    const float g = fminf(e, fminf(__fadd_rn(from_prev2, wx[j]), from_next2));
+    ch |= g < dj;
+    d[j] = g;
+    b = g;
   }
   return ch;
 }

@@ -23,22 +23,55 @@ constexpr uint64_t TMA_TIMEOUT_NS = 2000000000ull;  // 2 s
 // ------------------------------------------------------------------------------------------------------
 // Schedulers: what "activate a neighbour" and "finish a visit" mean.
 // ------------------------------------------------------------------------------------------------------
+// Per-warp counters, flushed to the queue header in batches (the header lines are shared by all warps).
+struct WarpStats {
+  uint32_t visits = 0, phases = 0, activations = 0, unflushed = 0;
+};
+
 struct QueueSched {
   Queue q;
   uint32_t* states;
-  // Idle -> queued; running -> running + re-run requested; queued -> unchanged.
-  __device__ __forceinline__ void activate(uint32_t tile) const {
-    if (tile >= q.total_tiles) { set_error(q, DERR_BAD_TILE, tile); return; }
-    const uint32_t old = atomicOr(&states[tile], ST_PENDING);
-    if (!(old & (ST_PENDING | ST_RUNNING))) queue_push(q, tile);
-  }
-  __device__ __forceinline__ void finish(uint32_t tile, uint32_t xor_bits, uint32_t nphase, uint32_t nact) const {
-    const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
-    if (old & ST_PENDING) queue_push(q, tile);  // a neighbour asked for a re-run while this visit ran
-    atomicAdd(&q.hdr->phases.v, nphase);
-    if (nact) atomicAdd(&q.hdr->activations.v, nact);
-    atomicAdd(&q.hdr->progress.v, 1u);
-    atomicSub(&q.hdr->pending.v, 1u);
+  // Warp-level end of a visit.  Lanes with `want` ask for a re-run of neighbour `item`: idle -> queued;
+  // running -> running with a re-run requested; queued -> unchanged.  Lane 31 clears RUNNING of the own
+  // tile (and sets / clears the xor_bits); a re-run requested meanwhile re-queues it.  `pending` moves by
+  // (pushes - 1) in one atomic performed before any push is visible; the visit that brings it to 0 ends
+  // the queue.
+  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item) const {
+    const int lane = threadIdx.x & 31;
+    bool push = false;
+    uint32_t item = 0;
+    if (want) {
+      if (want_item >= q.total_tiles) {
+        set_error(q, DERR_BAD_TILE, want_item);
+      } else {
+        const uint32_t old = atomicOr(&states[want_item], ST_PENDING);
+        push = !(old & (ST_PENDING | ST_RUNNING));
+        item = want_item;
+      }
+    }
+    if (lane == 31) {
+      const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
+      push = (old & ST_PENDING) != 0u;
+      item = tile;
+    }
+    const uint32_t m = __ballot_sync(~0u, push);
+    const uint32_t k = __popc(m);
+    uint32_t base = 0, last = 0;
+    if (lane == 0) {
+      if (k == 0) {
+        last = atomicSub(&q.hdr->pending.v, 1u) == 1u ? 1u : 0u;
+      } else {
+        if (k > 1) {
+          atomicAdd(&q.hdr->pending.v, k - 1u);
+          __threadfence();
+        }
+        base = atomicAdd(&q.hdr->tail.v, k);
+      }
+    }
+    __syncwarp();
+    base = __shfl_sync(~0u, base, 0);
+    if (push) slot_write(q, base + __popc(m & ((1u << lane) - 1u)), item);
+    if (__shfl_sync(~0u, last, 0)) signal_done_warp(q);
   }
 };
 
@@ -47,18 +80,39 @@ struct RoundSched {
   uint32_t* states;
   uint8_t* next_active;
   uint32_t* changed;
-  __device__ __forceinline__ void activate(uint32_t tile) const {
-    if (tile >= q.total_tiles) { set_error(q, DERR_BAD_TILE, tile); return; }
-    next_active[tile] = 1;
-    *(volatile uint32_t*)changed = 1u;
-  }
-  __device__ __forceinline__ void finish(uint32_t tile, uint32_t xor_bits, uint32_t nphase, uint32_t nact) const {
-    if (xor_bits) atomicXor(&states[tile], xor_bits);
-    atomicAdd(&q.hdr->phases.v, nphase);
-    if (nact) atomicAdd(&q.hdr->activations.v, nact);
-    atomicAdd(&q.hdr->progress.v, 1u);
+  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item) const {
+    if (want) {
+      if (want_item >= q.total_tiles) {
+        set_error(q, DERR_BAD_TILE, want_item);
+      } else {
+        next_active[want_item] = 1;
+        *(volatile uint32_t*)changed = 1u;
+      }
+    }
+    if ((threadIdx.x & 31) == 31 && xor_bits) atomicXor(&states[tile], xor_bits);
   }
 };
+
+// Adds a finished visit to the warp's counters; flushes `progress` every 16 visits (the watchdog and the
+// visit cap only need it approximately).
+__device__ __forceinline__ void count_visit(WarpStats& ws, const Queue& q, uint32_t nphase, uint32_t nact) {
+  ws.visits += 1;
+  ws.phases += nphase;
+  ws.activations += nact;
+  if (++ws.unflushed == 16) {
+    if ((threadIdx.x & 31) == 0) atomicAdd(&q.hdr->progress.v, ws.unflushed);
+    ws.unflushed = 0;
+  }
+}
+
+__device__ __forceinline__ void flush_stats(WarpStats& ws, const Queue& q) {
+  if ((threadIdx.x & 31) == 0) {
+    if (ws.unflushed) atomicAdd(&q.hdr->progress.v, ws.unflushed);
+    if (ws.phases) atomicAdd(&q.hdr->phases.v, ws.phases);
+    if (ws.activations) atomicAdd(&q.hdr->activations.v, ws.activations);
+  }
+  ws = WarpStats{};
+}
 
 __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
 
@@ -107,18 +161,20 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
 // ------------------------------------------------------------------------------------------------------
 // ns-mode visit (C4, w = sqrt(1 + g2 * dI2)), gray or rgb8.
 //
-// Layouts: "column" (lane = x, d[y]) and "row" (lane = y, d[x]).  A phase relaxes every edge of one
-// orientation with the two interleaved chains of sweep_line; the tile switches layout through the padded
-// buffer S.  The visit stops after a phase that changed nothing (and at least two phases), at which point
-// every edge of the tile and its halo is satisfied.  The halo is an upper bound of the neighbours' values
-// (values only decrease), so the visit never undershoots the fixpoint.  A neighbour is re-activated only if
-// some border pixel plus its edge weight is below the halo value it was compared against: the neighbour can
-// then still decrease; otherwise it cannot (its value is <= that halo value).
+// Layouts: "column" (lane = x, d[y]) and "row" (lane = y, d[x]); the tile switches layout through the padded
+// buffer S.  Each phase (sweep_phase) relaxes every internal edge of the tile and the halo edges of its own
+// axis; the halo edges of the other axis were relaxed by an earlier phase and stay satisfied, because tile
+// values only decrease while the halo is fixed.  So the visit stops at the first phase that changes nothing
+// once both layouts have run: every edge of the tile and its halo is then satisfied.  The halo is an upper
+// bound of the neighbours' values (values only decrease), so the visit never undershoots the fixpoint.  A
+// neighbour is re-activated only if some border pixel plus its edge weight is below the halo value it was
+// compared against: the neighbour can then still decrease; otherwise it cannot (its value is <= that halo
+// value).  Returns the number of phases and activations through *nph / *nact.
 // ------------------------------------------------------------------------------------------------------
 template <class Sched>
 __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
                                          uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
-                                         const Sched& sch) {
+                                         const Sched& sch, uint32_t* nph_out, uint32_t* nact_out) {
   const int lane = threadIdx.x & 31;
   const float INF = f_inf();
   const uint32_t local = tile - dd.tile_base;
@@ -129,19 +185,21 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   const bool seed = (old_state & ST_SEED) != 0;
   const bool rgb = dd.channels == 3;
   const float v = dd.v;
+  *nph_out = 0;
+  *nact_out = 0;
 
   stage_tile(sm, tm_img, tm_mask, rgb, seed, x0, y0);
 
   // Neighbour states: lane 0 left, 1 right, 2 top, 3 bottom.
+  const uint32_t nexist = (tx > 0 ? 1u : 0u) | (tx + 1 < dd.tiles_x ? 2u : 0u) | (ty > 0 ? 4u : 0u) |
+                          (ty + 1 < dd.tiles_y ? 8u : 0u);
+  const int nbx = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
+  const int nby = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
+  const uint32_t nb_tile = dd.tile_base + (uint32_t)(nby * dd.tiles_x + nbx);  // meaningful for lanes < 4
   uint32_t nvis;
   {
     bool vis = false;
-    if (lane < 4) {
-      const int nx = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
-      const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
-      if (nx >= 0 && ny >= 0 && nx < dd.tiles_x && ny < dd.tiles_y)
-        vis = (ld_volatile(&sch.states[dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx)]) & ST_VISITED) != 0;
-    }
+    if (lane < 4 && ((nexist >> lane) & 1u)) vis = (ld_volatile(&sch.states[nb_tile]) & ST_VISITED) != 0;
     nvis = __ballot_sync(~0u, vis);
   }
   __threadfence();  // acquire: distances were written before the VISITED bits / the activation we saw
@@ -149,12 +207,12 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Halo: column layout for top/bottom (lane = x), row layout for left/right (lane = y).
   float top = INF, bot = INF, lft = INF, rgt = INF;
   if (lane < vw) {
-    if (ty > 0) top = (nvis & 4u) ? dist_row(dd, y0 - 1)[x0 + lane] : v;
-    if (ty + 1 < dd.tiles_y) bot = (nvis & 8u) ? dist_row(dd, y0 + TILE)[x0 + lane] : v;
+    if (nexist & 4u) top = (nvis & 4u) ? dist_row(dd, y0 - 1)[x0 + lane] : v;
+    if (nexist & 8u) bot = (nvis & 8u) ? dist_row(dd, y0 + TILE)[x0 + lane] : v;
   }
   if (lane < vh) {
-    if (tx > 0) lft = (nvis & 1u) ? dist_row(dd, y0 + lane)[x0 - 1] : v;
-    if (tx + 1 < dd.tiles_x) rgt = (nvis & 2u) ? dist_row(dd, y0 + lane)[x0 + TILE] : v;
+    if (nexist & 1u) lft = (nvis & 1u) ? dist_row(dd, y0 + lane)[x0 - 1] : v;
+    if (nexist & 2u) rgt = (nvis & 2u) ? dist_row(dd, y0 + lane)[x0 + TILE] : v;
   }
 
   // Tile distances in column layout.
@@ -166,34 +224,49 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 
   if (!tma_wait(sm, parity, sch.q, tile)) return;
 
-  // Edge weights.  wv[k]: edge (row k-1, row k) of column `lane`; horizontal weights go through S.
+  // Edge weights in both layouts.  Column layout (lane = x): wv_c[k] edge (row k-1, row k) of the column,
+  // wh_c[y] edge (column x-1, column x) on row y.  Row layout (lane = y): wh_r[k] edge (column k-1, column k)
+  // of the row, wv_r[x] edge (row y-1, row y) on column x.  Edges that touch a pixel outside the image are INF.
   const float g2 = dd.g2;
-  float wv[TILE + 1];
+  float wv_c[TILE + 1], wh_c[TILE];
   {
     const uint8_t* box = sm.img;
     uint32_t pprev = box_pix(box, rgb, 0, lane);
 #pragma unroll
     for (int r = 1; r <= TILE + 1; ++r) {
       const uint32_t pcur = box_pix(box, rgb, r, lane);
-      wv[r - 1] = ns_weight(pprev, pcur, g2);
-      if (r <= TILE) sm.S[(r - 1) * S_STRIDE + lane] = ns_weight(box_pix(box, rgb, r, lane - 1), pcur, g2);
+      wv_c[r - 1] = ns_weight(pprev, pcur, g2);
+      if (r <= TILE) wh_c[r - 1] = ns_weight(box_pix(box, rgb, r, lane - 1), pcur, g2);
       pprev = pcur;
     }
   }
-  // Edge (x = 31, x = 32) of row `lane`.
   const float er = ns_weight(box_pix(sm.img, rgb, lane + 1, TILE - 1), box_pix(sm.img, rgb, lane + 1, TILE), g2);
 #pragma unroll
   for (int k = 0; k <= TILE; ++k)
-    if (lane >= vw || (k < TILE ? k >= vh : TILE - 1 >= vh)) wv[k] = INF;
-  __syncwarp();
-  float wh[TILE + 1];
+    if (lane >= vw || (k < TILE ? k >= vh : TILE - 1 >= vh)) wv_c[k] = INF;
 #pragma unroll
-  for (int k = 0; k < TILE; ++k) wh[k] = sm.S[lane * S_STRIDE + k];
-  wh[TILE] = er;
+  for (int y = 0; y < TILE; ++y)
+    if (lane >= vw || y >= vh) wh_c[y] = INF;
+  float wh_r[TILE + 1], wv_r[TILE];
+#pragma unroll
+  for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = wh_c[y];
+  __syncwarp();
+#pragma unroll
+  for (int x = 0; x < TILE; ++x) wh_r[x] = sm.S[lane * S_STRIDE + x];
+  wh_r[TILE] = er;
+  __syncwarp();
+#pragma unroll
+  for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = wv_c[y];
+  __syncwarp();
+#pragma unroll
+  for (int x = 0; x < TILE; ++x) wv_r[x] = sm.S[lane * S_STRIDE + x];
+  __syncwarp();
 #pragma unroll
   for (int k = 0; k <= TILE; ++k)
-    if (lane >= vh || (k < TILE ? k >= vw : TILE - 1 >= vw)) wh[k] = INF;
-  __syncwarp();
+    if (lane >= vh || (k < TILE ? k >= vw : TILE - 1 >= vw)) wh_r[k] = INF;
+#pragma unroll
+  for (int x = 0; x < TILE; ++x)
+    if (lane >= vh || x >= vw) wv_r[x] = INF;
 
   if (first) {
 #pragma unroll
@@ -209,13 +282,15 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   }
 
   // Local fixpoint.
-  bool any = false;
+  bool any = false, ran_col = false, ran_row = false;
   uint32_t nph = 0;
   bool col = true;
   for (;;) {
-    bool ch = col ? sweep_line(d, wv, top, bot) : sweep_line(d, wh, lft, rgt);
+    bool ch = col ? sweep_phase(d, wv_c, wh_c, top, bot) : sweep_phase(d, wh_r, wv_r, lft, rgt);
     ch = __any_sync(~0u, ch);
     any |= ch;
+    ran_col |= col;
+    ran_row |= !col;
     ++nph;
     if (col) {
 #pragma unroll
@@ -225,7 +300,7 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
       for (int x = 0; x < TILE; ++x) sm.S[lane * S_STRIDE + x] = d[x];
     }
     __syncwarp();
-    if ((!ch && nph >= 2) || nph >= (uint32_t)PHASE_LIMIT) break;
+    if ((!ch && ran_col && ran_row) || nph >= (uint32_t)PHASE_LIMIT) break;
     if (col) {
 #pragma unroll
       for (int x = 0; x < TILE; ++x) d[x] = sm.S[lane * S_STRIDE + x];
@@ -243,13 +318,11 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   if (any || seed) {
     const float dt = sm.S[lane], db = sm.S[(TILE - 1) * S_STRIDE + lane];
     const float dl = sm.S[lane * S_STRIDE], dr = sm.S[lane * S_STRIDE + TILE - 1];
-    act |= __any_sync(~0u, __fadd_rn(dl, wh[0]) < lft) ? 1u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dr, wh[TILE]) < rgt) ? 2u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dt, wv[0]) < top) ? 4u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(db, wv[TILE]) < bot) ? 8u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dl, wh_r[0]) < lft) ? 1u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dr, wh_r[TILE]) < rgt) ? 2u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dt, wv_c[0]) < top) ? 4u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(db, wv_c[TILE]) < bot) ? 8u : 0u;
     // A missing neighbour has an INF halo, and fl(d + w) < INF holds for any finite d: mask by existence.
-    const uint32_t nexist = (tx > 0 ? 1u : 0u) | (tx + 1 < dd.tiles_x ? 2u : 0u) | (ty > 0 ? 4u : 0u) |
-                            (ty + 1 < dd.tiles_y ? 8u : 0u);
     act &= nexist;
   }
 
@@ -263,14 +336,9 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   }
   __threadfence();  // release: distances before activations and before the VISITED bit
   __syncwarp();
-  if (lane < 4 && ((act >> lane) & 1u)) {
-    const int nx = tx + (lane == 0 ? -1 : lane == 1 ? 1 : 0);
-    const int ny = ty + (lane == 2 ? -1 : lane == 3 ? 1 : 0);
-    sch.activate(dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx));
-  }
-  __syncwarp();
-  if (lane == 0)
-    sch.finish(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), nph, (uint32_t)__popc(act));
+  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), lane < 4 && ((act >> lane) & 1u), nb_tile);
+  *nph_out = nph;
+  *nact_out = (uint32_t)__popc(act);
 }
 
 // ------------------------------------------------------------------------------------------------------
@@ -299,7 +367,9 @@ __device__ __forceinline__ float ref_min3(float cur, float da, float db, float d
 template <bool FMA, class Sched>
 __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
                                           uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
-                                          const Sched& sch) {
+                                          const Sched& sch, uint32_t* nph_out, uint32_t* nact_out) {
+  *nph_out = 0;
+  *nact_out = 0;
   const int lane = threadIdx.x & 31;
   const float INF = f_inf();
   const uint32_t local = tile - dd.tile_base;
@@ -534,26 +604,29 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   }
   __threadfence();
   __syncwarp();
-  if (lane < 8 && ((act >> lane) & 1u))
-    sch.activate(dd.tile_base + (uint32_t)((ty + ndy[lane]) * dd.tiles_x + tx + ndx[lane]));
-  __syncwarp();
-  if (lane == 0)
-    sch.finish(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), nph, (uint32_t)__popc(act));
+  const bool want = lane < 8 && ((act >> lane) & 1u);
+  const uint32_t item = want ? dd.tile_base + (uint32_t)((ty + ndy[lane]) * dd.tiles_x + tx + ndx[lane]) : 0u;
+  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), want, item);
+  *nph_out = nph;
+  *nact_out = (uint32_t)__popc(act);
 }
 
 // MODE is fixed per kernel instantiation: a launch covers images of one weight mode only, so the
 // register allocation of the ns-mode kernel is not inflated by the ref-mode code.
 template <int MODE, class Sched>
 __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap* tmaps, uint32_t img, uint32_t tile,
-                                           uint32_t old_state, WarpSmem& sm, uint32_t& parity, const Sched& sch) {
+                                           uint32_t old_state, WarpSmem& sm, uint32_t& parity, const Sched& sch,
+                                           WarpStats& ws) {
   const CUtensorMap* tm_img = tmaps + 2 * img;
   const CUtensorMap* tm_mask = tmaps + 2 * img + 1;
+  uint32_t nph, nact;
   if (MODE == MODE_NS)
-    visit_ns(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+    visit_ns(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
   else if (dd.ref_fma)
-    visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+    visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
   else
-    visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch);
+    visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
+  count_visit(ws, sch.q, nph, nact);
 }
 
 __device__ __forceinline__ WarpSmem& warp_slot(uint8_t* smem_raw) {

@@ -56,6 +56,7 @@ typedef struct dtb_context_s* dtb_context;
 #define DTB_FLAG_ASYNC 0x1u       /* device images only: return after enqueueing; call dtb_sync() for the status */
 #define DTB_FLAG_ROUNDS 0x2u      /* plain per-image path: host-driven rounds over active tiles */
 #define DTB_FLAG_REF_NO_FMA 0x4u  /* ref-mode: round l_eucl*d and l_grad*|dI| separately instead of contracting */
+#define DTB_FLAG_TIMING 0x8u      /* record CUDA events around the tile kernel; dtb_stats.kernel_ms */
 
 /* Counters of the last synchronous call (or of the call waited for by dtb_sync). */
 typedef struct dtb_stats {
@@ -66,6 +67,7 @@ typedef struct dtb_stats {
   uint64_t rounds;        /* host rounds (DTB_FLAG_ROUNDS), else 1 */
   uint32_t device_error;  /* 0, or the device error code */
   uint32_t device_error_info;
+  double kernel_ms;       /* DTB_FLAG_TIMING: device time of the tile kernel(s) of the call, else 0 */
 } dtb_stats;
 
 DTB_API int32_t dtb_abi_version(void);
