@@ -25,7 +25,7 @@ STATUS_NAMES = {
 # Every symbol include/dtb.h declares (checked by the CPU test suite).
 DTB_SYMBOLS = [
     "dtb_abi_version", "dtb_status_string", "dtb_context_create", "dtb_context_destroy", "dtb_context_message",
-    "dtb_last_stats", "dtb_sync", "dtb_gdt_ref", "dtb_gdt", "dtb_gdt_batch", "dtb_host_to_device",
+    "dtb_last_stats", "dtb_sync", "dtb_gdt_ref", "dtb_gdt", "dtb_gdt_batch", "dtb_gdt_noalloc", "dtb_host_to_device",
     "dtb_device_to_host",
 ]
 
@@ -95,6 +95,8 @@ def lib():
         L.dtb_gdt.argtypes = [P, IMG, IMG, IMG, F, F, U32, P]
         L.dtb_gdt_batch.restype = I32
         L.dtb_gdt_batch.argtypes = [P, I32, IMG, IMG, IMG, ctypes.POINTER(F), F, U32, P]
+        L.dtb_gdt_noalloc.restype = I32
+        L.dtb_gdt_noalloc.argtypes = [IMG, IMG, IMG, F, F, P]
         L.dtb_host_to_device.restype = I32
         L.dtb_host_to_device.argtypes = [IMG, IMG, P]
         L.dtb_device_to_host.restype = I32

@@ -103,6 +103,20 @@ DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_imag
 DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
                                  const dtb_image* dists, const float* gammas, float v, uint32_t flags, void* stream);
 
+/* Allocation-free dtb_gdt for one image; no counterpart in the reference.
+ * For callers that must not allocate device memory behind their own allocator: a host that owns all device
+ * memory through its own pool or budget, or a loop that cannot afford the device-wide synchronisation of
+ * cudaMalloc / cudaFree.  No context: the scratch is a fixed array in the library's device memory (about
+ * 322 KB on every GPU that loads the library, held until exit), so the image may have at most 16384 tiles of
+ * 32 x 32 pixels (e.g. 4096 x 4096); larger images return DTB_ERR_CAPACITY.  img, mask and dist must be device
+ * memory, img and mask with 16-byte aligned buffer and pitch, dist with 4-byte alignment (no staging copies);
+ * otherwise DTB_ERR_INVALID_ARG.  Synchronous: returns after the map is written.  The first call on a device
+ * does a one-time set-up with that device current (symbol address, driver entry point, kernel attributes);
+ * make that first call before any stream capture.  Every call reuses the same array and clears what must start
+ * at zero; calls that overlap on the GPU (other threads or streams) race on it and must be serialised. */
+DTB_API dtb_status dtb_gdt_noalloc(const dtb_image* img, const dtb_image* mask, const dtb_image* dist, float gamma,
+                                   float v, void* stream);
+
 /* Host <-> device copies of a pitched image, reference dt::host_to_device / dt::device_to_host
  * (dt/include/dt/transfert.hpp:13-15, dt/src/transfert.cpp:10-28).  Synchronous when stream is NULL. */
 DTB_API dtb_status dtb_host_to_device(const dtb_image* src, const dtb_image* dst, void* stream);
