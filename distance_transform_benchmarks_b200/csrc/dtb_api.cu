@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -142,7 +143,12 @@ __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__
 namespace {
 
 constexpr int PERSIST_WPC = 4;
-constexpr int PERSIST_MINB = 2;
+constexpr int PERSIST_MINB_REF = 2;
+// ns-mode persistent kernel variants: CTAs (of PERSIST_WPC warps) per SM, i.e. registers per thread
+// 255 / 168 / 128.  The choice is a tuning knob (dtb_context_set_tuning), default NS_VARIANT_DEFAULT.
+constexpr int NS_VARIANTS = 3;
+constexpr int NS_VARIANT_MINB[NS_VARIANTS] = {2, 3, 4};
+constexpr int NS_VARIANT_DEFAULT = 0;
 constexpr int ROUND_WPC = 4;
 constexpr size_t SMEM_SLOT = sizeof(WarpSmem);
 constexpr size_t PERSIST_SMEM = PERSIST_WPC * SMEM_SLOT + 128;
@@ -161,7 +167,10 @@ uint32_t next_pow2(uint32_t x) {
 struct dtb_context_s {
   int device = 0;
   int num_sms = 0;
-  int persist_blocks_per_sm[2] = {0, 0};  // per weight mode
+  int persist_blocks_per_sm[2] = {0, 0};  // per weight mode (ns: of the selected variant)
+  const void* ns_fn[NS_VARIANTS] = {};
+  int ns_blocks_per_sm[NS_VARIANTS] = {};
+  int ns_variant = NS_VARIANT_DEFAULT;
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   void* dscratch = nullptr;
   size_t dscratch_size = 0;
@@ -414,10 +423,12 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], stream));
-      if (mode == MODE_NS)
-        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
-      else
-        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>, ddesc, dtm, states, q));
+      if (mode == MODE_NS) {
+        void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
+        DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->ns_fn[ctx->ns_variant], args));
+      } else {
+        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB_REF>, ddesc, dtm, states, q));
+      }
       if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], stream));
     } else {
       DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
@@ -528,8 +539,24 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
     delete ctx;
     return DTB_ERR_NO_DEVICE;
   }
-  const void* kp[2] = {(const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, PERSIST_MINB>,
-                        (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB>};
+  ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[0]>;
+  ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[1]>;
+  ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[2]>;
+  for (int k = 0; k < NS_VARIANTS; ++k) {
+    if (cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], PERSIST_WPC * 32,
+                                                      PERSIST_SMEM) != cudaSuccess ||
+        ctx->ns_blocks_per_sm[k] < 1) {
+      delete ctx;
+      return DTB_ERR_NO_DEVICE;
+    }
+  }
+  if (const char* e = getenv("DTB_NS_VARIANT")) {
+    const int k = atoi(e);
+    if (k >= 0 && k < NS_VARIANTS) ctx->ns_variant = k;
+  }
+  const void* kp[2] = {ctx->ns_fn[ctx->ns_variant],
+                        (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB_REF>};
   const void* kr[2] = {(const void*)ggdt_round<MODE_NS, ROUND_WPC>, (const void*)ggdt_round<MODE_REF, ROUND_WPC>};
   for (int m = 0; m < 2; ++m) {
     if (cudaFuncSetAttribute(kp[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||

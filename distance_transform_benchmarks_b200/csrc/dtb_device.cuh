@@ -82,16 +82,17 @@ struct Queue {
   uint32_t total_tiles;     // tile ids are < total_tiles
 };
 
-// Per-warp shared memory slot.
+// Per-warp shared memory slot (13 KB: 16 warps per SM fit in 228 KB).
+constexpr int W_STRIDE = TILE + 1;  // weight / tile buffers: 33 floats per row, conflict-free in both layouts
 struct alignas(128) WarpSmem {
-  uint8_t img[IMG_BOX_ROWS * IMG_BOX_RGB];   // TMA destination (gray uses IMG_BOX_ROWS x 64)
-  uint8_t mask[TILE * TILE];                 // TMA destination for seed masks
-  float S[TILE * S_STRIDE];                  // transpose / final tile values
-  float er[TILE];                            // weights of the edges x=31 -> x=32 per row
-  float hl[TILE + 2];                        // ref-mode: halo column x = -1 (rows -1..32)
-  float hr[TILE + 2];                        // ref-mode: halo column x = 32
+  uint8_t img[IMG_BOX_ROWS * IMG_BOX_RGB];   // TMA destination of the image box (gray uses IMG_BOX_ROWS x 64); once
+                                             // the weights are computed, the tile buffer B[y * 33 + x]
+  float Wh[TILE * W_STRIDE];                 // ns-mode: Wh[y * 33 + x] = weight of edge (x-1, x) on row y, x = 0..32
+  float Wv[(TILE + 1) * W_STRIDE];           // ns-mode: Wv[y * 33 + x] = weight of edge (y-1, y) on column x, y = 0..32;
+                                             // its first 1 KB receives the seed-mask TMA box before the weights
   uint64_t bar;                              // TMA mbarrier
 };
+__device__ __forceinline__ uint8_t* mask_box(WarpSmem& sm) { return reinterpret_cast<uint8_t*>(sm.Wv); }
 
 // ------------------------------------------------------------------------------------------------------
 // PTX helpers

@@ -146,7 +146,7 @@ __device__ __forceinline__ void stage_tile(WarpSmem& sm, const CUtensorMap* tm_i
     const uint32_t bytes = (rgb ? IMG_BOX_RGB : IMG_BOX_GRAY) * IMG_BOX_ROWS + (with_mask ? TILE * TILE : 0);
     mbar_arrive_expect_tx(&sm.bar, bytes);
     tma_load_2d(sm.img, tm_img, rgb ? 3 * x0 - 16 : x0 - 16, y0 - 1, &sm.bar);
-    if (with_mask) tma_load_2d(sm.mask, tm_mask, x0, y0, &sm.bar);
+    if (with_mask) tma_load_2d(mask_box(sm), tm_mask, x0, y0, &sm.bar);
   }
 }
 
@@ -161,15 +161,20 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
 // ------------------------------------------------------------------------------------------------------
 // ns-mode visit (C4, w = sqrt(1 + g2 * dI2)), gray or rgb8.
 //
-// Layouts: "column" (lane = x, d[y]) and "row" (lane = y, d[x]); the tile switches layout through the padded
-// buffer S.  Each phase (sweep_phase) relaxes every internal edge of the tile and the halo edges of its own
-// axis; the halo edges of the other axis were relaxed by an earlier phase and stay satisfied, because tile
-// values only decrease while the halo is fixed.  So the visit stops at the first phase that changes nothing
-// once both layouts have run: every edge of the tile and its halo is then satisfied.  The halo is an upper
-// bound of the neighbours' values (values only decrease), so the visit never undershoots the fixpoint.  A
-// neighbour is re-activated only if some border pixel plus its edge weight is below the halo value it was
-// compared against: the neighbour can then still decrease; otherwise it cannot (its value is <= that halo
-// value).  Returns the number of phases and activations through *nph / *nact.
+// Layouts: "column" (lane = x, d[y]) and "row" (lane = y, d[x]).  Each phase (sweep_phase) relaxes every
+// internal edge of the tile and the halo edges of its own axis; the halo edges of the other axis were relaxed
+// by an earlier phase and stay satisfied, because tile values only decrease while the halo is fixed.  So the
+// visit stops at the first phase that changes nothing once both layouts have run: every edge of the tile and
+// its halo is then satisfied.  The halo is an upper bound of the neighbours' values (values only decrease;
+// never-visited neighbours read as v), so the visit never undershoots the fixpoint.  A neighbour is
+// re-activated only if some border pixel plus its edge weight is below the halo value it was compared with.
+//
+// One code path serves both layouts (the phase loop is small enough to stay in the instruction cache): the
+// weights live in shared memory as Wh / Wv (stride 33, conflict-free for a lane-per-row and a lane-per-column
+// read alike) and are loaded into registers for the phase's layout; the tile changes layout through B.
+// Element k of lane l of the current layout is at [k * sa + l * sb] of the plain row-major arrays
+// (column layout: sa = 33, sb = 1; row layout: sa = 1, sb = 33).
+// Returns the number of phases and activations through *nph / *nact.
 // ------------------------------------------------------------------------------------------------------
 template <class Sched>
 __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
@@ -224,91 +229,73 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 
   if (!tma_wait(sm, parity, sch.q, tile)) return;
 
-  // Edge weights in both layouts.  Column layout (lane = x): wv_c[k] edge (row k-1, row k) of the column,
-  // wh_c[y] edge (column x-1, column x) on row y.  Row layout (lane = y): wh_r[k] edge (column k-1, column k)
-  // of the row, wv_r[x] edge (row y-1, row y) on column x.  Edges that touch a pixel outside the image are INF.
-  const float g2 = dd.g2;
-  float wv_c[TILE + 1], wh_c[TILE];
-  {
-    const uint8_t* box = sm.img;
-    uint32_t pprev = box_pix(box, rgb, 0, lane);
-#pragma unroll
-    for (int r = 1; r <= TILE + 1; ++r) {
-      const uint32_t pcur = box_pix(box, rgb, r, lane);
-      wv_c[r - 1] = ns_weight(pprev, pcur, g2);
-      if (r <= TILE) wh_c[r - 1] = ns_weight(box_pix(box, rgb, r, lane - 1), pcur, g2);
-      pprev = pcur;
-    }
-  }
-  const float er = ns_weight(box_pix(sm.img, rgb, lane + 1, TILE - 1), box_pix(sm.img, rgb, lane + 1, TILE), g2);
-#pragma unroll
-  for (int k = 0; k <= TILE; ++k)
-    if (lane >= vw || (k < TILE ? k >= vh : TILE - 1 >= vh)) wv_c[k] = INF;
-#pragma unroll
-  for (int y = 0; y < TILE; ++y)
-    if (lane >= vw || y >= vh) wh_c[y] = INF;
-  float wh_r[TILE + 1], wv_r[TILE];
-#pragma unroll
-  for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = wh_c[y];
-  __syncwarp();
-#pragma unroll
-  for (int x = 0; x < TILE; ++x) wh_r[x] = sm.S[lane * S_STRIDE + x];
-  wh_r[TILE] = er;
-  __syncwarp();
-#pragma unroll
-  for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = wv_c[y];
-  __syncwarp();
-#pragma unroll
-  for (int x = 0; x < TILE; ++x) wv_r[x] = sm.S[lane * S_STRIDE + x];
-  __syncwarp();
-#pragma unroll
-  for (int k = 0; k <= TILE; ++k)
-    if (lane >= vh || (k < TILE ? k >= vw : TILE - 1 >= vw)) wh_r[k] = INF;
-#pragma unroll
-  for (int x = 0; x < TILE; ++x)
-    if (lane >= vh || x >= vw) wv_r[x] = INF;
-
+  // Seeds first: the mask box shares memory with Wv.
   if (first) {
 #pragma unroll
     for (int y = 0; y < TILE; ++y) {
       const bool in = lane < vw && y < vh;
-      const bool s = seed && sm.mask[y * TILE + lane] != 0;
+      const bool s = seed && mask_box(sm)[y * TILE + lane] != 0;
       d[y] = in ? (s ? 0.0f : v) : INF;
     }
   } else if (seed) {
 #pragma unroll
     for (int y = 0; y < TILE; ++y)
-      if (lane < vw && y < vh && sm.mask[y * TILE + lane] != 0) d[y] = 0.0f;
+      if (lane < vw && y < vh && mask_box(sm)[y * TILE + lane] != 0) d[y] = 0.0f;
   }
+  __syncwarp();
 
-  // Local fixpoint.
-  bool any = false, ran_col = false, ran_row = false;
+  // Edge weights into Wh / Wv (computed in column layout, lane = x).  Edges touching a pixel outside the image
+  // are INF.
+  {
+    const float g2 = dd.g2;
+    const uint8_t* box = sm.img;
+    uint32_t pprev = box_pix(box, rgb, 0, lane);
+#pragma unroll 1
+    for (int y = 0; y <= TILE; ++y) {  // edge (y-1, y); y == 32 is the bottom halo edge
+      const uint32_t pcur = box_pix(box, rgb, y + 1, lane);
+      float w = ns_weight(pprev, pcur, g2);
+      if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
+      sm.Wv[y * W_STRIDE + lane] = w;
+      if (y < TILE) {
+        float wx = ns_weight(box_pix(box, rgb, y + 1, lane - 1), pcur, g2);
+        if (lane >= vw || y >= vh) wx = INF;
+        sm.Wh[y * W_STRIDE + lane] = wx;
+      }
+      pprev = pcur;
+    }
+    // Edge (x = 31, x = 32) of row `lane`.
+    float er = ns_weight(box_pix(box, rgb, lane + 1, TILE - 1), box_pix(box, rgb, lane + 1, TILE), g2);
+    if (lane >= vh || TILE - 1 >= vw) er = INF;
+    sm.Wh[lane * W_STRIDE + TILE] = er;
+  }
+  __syncwarp();
+
+  // Local fixpoint.  B overlays the image box, which is no longer needed.
+  float* B = reinterpret_cast<float*>(sm.img);
+  bool any = false, ran_col = false, ran_row = false, col = true;
   uint32_t nph = 0;
-  bool col = true;
   for (;;) {
-    bool ch = col ? sweep_phase(d, wv_c, wh_c, top, bot) : sweep_phase(d, wh_r, wv_r, lft, rgt);
+    const int sa = col ? W_STRIDE : 1, sb = col ? 1 : W_STRIDE;
+    const float* Wc = col ? sm.Wv : sm.Wh;  // chain edges of the layout
+    const float* Wx = col ? sm.Wh : sm.Wv;  // cross edges
+    float wc[TILE + 1], wx[TILE];
+#pragma unroll
+    for (int k = 0; k <= TILE; ++k) wc[k] = Wc[k * sa + lane * sb];
+#pragma unroll
+    for (int k = 0; k < TILE; ++k) wx[k] = Wx[k * sa + lane * sb];
+    bool ch = sweep_phase(d, wc, wx, col ? top : lft, col ? bot : rgt);
     ch = __any_sync(~0u, ch);
     any |= ch;
     ran_col |= col;
     ran_row |= !col;
     ++nph;
-    if (col) {
 #pragma unroll
-      for (int y = 0; y < TILE; ++y) sm.S[y * S_STRIDE + lane] = d[y];
-    } else {
-#pragma unroll
-      for (int x = 0; x < TILE; ++x) sm.S[lane * S_STRIDE + x] = d[x];
-    }
+    for (int k = 0; k < TILE; ++k) B[k * sa + lane * sb] = d[k];
     __syncwarp();
     if ((!ch && ran_col && ran_row) || nph >= (uint32_t)PHASE_LIMIT) break;
-    if (col) {
-#pragma unroll
-      for (int x = 0; x < TILE; ++x) d[x] = sm.S[lane * S_STRIDE + x];
-    } else {
-#pragma unroll
-      for (int y = 0; y < TILE; ++y) d[y] = sm.S[y * S_STRIDE + lane];
-    }
     col = !col;
+#pragma unroll
+    for (int k = 0; k < TILE; ++k) d[k] = B[k * sb + lane * sa];  // the other layout
     __syncwarp();
   }
   if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);
@@ -316,12 +303,14 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Neighbours that can still decrease (bit 0 left, 1 right, 2 top, 3 bottom).
   uint32_t act = 0;
   if (any || seed) {
-    const float dt = sm.S[lane], db = sm.S[(TILE - 1) * S_STRIDE + lane];
-    const float dl = sm.S[lane * S_STRIDE], dr = sm.S[lane * S_STRIDE + TILE - 1];
-    act |= __any_sync(~0u, __fadd_rn(dl, wh_r[0]) < lft) ? 1u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dr, wh_r[TILE]) < rgt) ? 2u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dt, wv_c[0]) < top) ? 4u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(db, wv_c[TILE]) < bot) ? 8u : 0u;
+    const float dt = B[lane], db = B[(TILE - 1) * W_STRIDE + lane];               // column layout
+    const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];      // row layout
+    const float wt = sm.Wv[lane], wb = sm.Wv[TILE * W_STRIDE + lane];
+    const float wl = sm.Wh[lane * W_STRIDE], wr = sm.Wh[lane * W_STRIDE + TILE];
+    act |= __any_sync(~0u, __fadd_rn(dl, wl) < lft) ? 1u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dr, wr) < rgt) ? 2u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(dt, wt) < top) ? 4u : 0u;
+    act |= __any_sync(~0u, __fadd_rn(db, wb) < bot) ? 8u : 0u;
     // A missing neighbour has an INF halo, and fl(d + w) < INF holds for any finite d: mask by existence.
     act &= nexist;
   }
@@ -329,9 +318,9 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Write back (column layout: each row is one coalesced 128-byte store).
   if (any || first) {
     if (lane < vw) {
-#pragma unroll
+#pragma unroll 4
       for (int y = 0; y < TILE; ++y)
-        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = sm.S[y * S_STRIDE + lane];
+        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = B[y * W_STRIDE + lane];
     }
   }
   __threadfence();  // release: distances before activations and before the VISITED bit
@@ -400,10 +389,10 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   __threadfence();
 
   // Halo rows / columns in shared memory, index = coordinate + 1 (corners appear in both).
-  float* ht = sm.S;                 // top row   (y0 - 1), x = -1..32
-  float* hb = sm.S + 40;            // bottom row (y0 + 32)
-  float* hl = sm.hl;                // left column (x0 - 1), y = -1..32
-  float* hr = sm.hr;                // right column (x0 + 32)
+  float* ht = sm.Wh;                // top row   (y0 - 1), x = -1..32
+  float* hb = sm.Wh + 40;           // bottom row (y0 + 32)
+  float* hl = sm.Wv + 256;          // left column (x0 - 1), y = -1..32 (after the 1 KB seed-mask box)
+  float* hr = sm.Wv + 300;          // right column (x0 + 32)
   auto halo_val = [&](int k, int gx, int gy) -> float {  // neighbour k's pixel (gx, gy)
     if (!((nexist >> k) & 1u)) return INF;
     if (gx >= dd.width || gy >= dd.height) return INF;
@@ -431,7 +420,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   if (!tma_wait(sm, parity, sch.q, tile)) return;
 
   // Padded copy of the image box: pimg[r * 36 + c + 1] = pixel (tile column c, box row r), c = -1..32.
-  uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.S + 96);  // 34 * 36 = 1224 bytes after the halo rows
+  uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.Wh + 96);  // 34 * 36 = 1224 bytes after the halo rows
   for (int i = lane; i < IMG_BOX_ROWS * PIMG_STRIDE; i += 32) {
     const int r = i / PIMG_STRIDE, c = i % PIMG_STRIDE;
     pimg[i] = (c < TILE + 2) ? sm.img[r * IMG_BOX_GRAY + 15 + c] : 0;
@@ -441,12 +430,12 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
 #pragma unroll
     for (int y = 0; y < TILE; ++y) {
       const bool in = lane < vw && y < vh;
-      d[y] = in ? ((seed && sm.mask[y * TILE + lane] != 0) ? 0.0f : v) : INF;
+      d[y] = in ? ((seed && mask_box(sm)[y * TILE + lane] != 0) ? 0.0f : v) : INF;
     }
   } else if (seed) {
 #pragma unroll
     for (int y = 0; y < TILE; ++y)
-      if (lane < vw && y < vh && sm.mask[y * TILE + lane] != 0) d[y] = 0.0f;
+      if (lane < vw && y < vh && mask_box(sm)[y * TILE + lane] != 0) d[y] = 0.0f;
   }
   __syncwarp();
 

@@ -54,9 +54,6 @@ __device__ __forceinline__ const ImgDesc* na_desc() {
 __device__ __forceinline__ const CUtensorMap* na_tmaps() {
   return reinterpret_cast<const CUtensorMap*>(g_noalloc_scratch + OFF_TMAP);
 }
-__device__ __forceinline__ const uint32_t* na_base() {
-  return reinterpret_cast<const uint32_t*>(g_noalloc_scratch + OFF_BASE);
-}
 __device__ __forceinline__ uint32_t* na_states() { return reinterpret_cast<uint32_t*>(g_noalloc_scratch + OFF_STATES); }
 __device__ __forceinline__ Queue na_queue(uint32_t max_visits, uint32_t tiles) {
   return Queue{na_hdr(), reinterpret_cast<uint32_t*>(g_noalloc_scratch + OFF_RING), NOALLOC_RING - 1, NOALLOC_TIMEOUT_NS,
