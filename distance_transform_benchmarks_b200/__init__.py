@@ -16,12 +16,13 @@ import numpy as np
 import torch
 
 from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_FLAG_TIMING, DTB_GPU, DtbError,
-                      DtbImage, DtbStats, lib)
+                      DtbImage, DtbStats, DtbTuning, lib)
 
 __all__ = [
     "Context", "DtbError", "default_context", "generalised_distance_transform",
     "generalised_distance_transform_blocks", "generalised_distance_transform_task", "geodesic_distance_transform",
-    "geodesic_distance_transform_batch", "host_to_device", "device_to_host", "image_view", "DEFAULT_V",
+    "geodesic_distance_transform_batch", "host_to_device", "device_to_host", "image_view", "DEFAULT_V", "BatchPlan",
+    "pitched_empty", "pitched_from",
 ]
 
 DEFAULT_V = 1e10  # reference default, generalised_distance_transform.hpp:8
@@ -51,6 +52,14 @@ class Context:
         s = DtbStats()
         self.check(lib().dtb_last_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in DtbStats._fields_}
+
+    def set_tuning(self, ctas_per_sm=0, grid_percent=0):
+        self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(DtbTuning(ctas_per_sm, grid_percent))))
+
+    def get_tuning(self):
+        t = DtbTuning()
+        self.check(lib().dtb_context_get_tuning(self._h, ctypes.byref(t)))
+        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent}
 
     def sync(self, stream=None):
         self.check(lib().dtb_sync(self._h, ctypes.c_void_p(_stream_ptr(stream))))
@@ -110,6 +119,30 @@ def image_view(t, elem_size=None):
     pitch = t.stride(0) * t.element_size() if h > 1 else w * es
     kind = DTB_GPU if t.is_cuda else DTB_CPU
     return DtbImage(t.data_ptr() if t.numel() else None, w, h, pitch, es, kind)
+
+
+PITCH_ALIGN = 128  # bytes; cudaMallocPitch-style rows, as the reference's GPU image2d (image2d_data_gpu.hpp:28)
+
+
+def pitched_empty(height, width, channels=1, dtype=torch.uint8, device="cuda"):
+    """Uninitialised [H, W] (or [H, W, C]) tensor whose rows start every PITCH_ALIGN bytes: the layout the TMA
+    path reads without staging (the reference allocates GPU images the same way)."""
+    es = torch.empty((), dtype=dtype).element_size()
+    row = width * channels * es
+    pitch_elems = (-(-max(row, 1) // PITCH_ALIGN) * PITCH_ALIGN) // es
+    store = torch.empty((max(height, 1), pitch_elems), dtype=dtype, device=device)
+    if channels == 1:
+        return store[:height, :width]
+    return torch.as_strided(store, (height, width, channels), (pitch_elems, channels, 1))
+
+
+def pitched_from(arr, device="cuda"):
+    """Copy of a [H, W] / [H, W, C] array into a pitched device tensor."""
+    t = _as_tensor(arr)
+    c = t.shape[2] if t.dim() == 3 else 1
+    out = pitched_empty(t.shape[0], t.shape[1], c, t.dtype, device)
+    out.copy_(t)
+    return out
 
 
 def _as_tensor(x):
@@ -220,3 +253,51 @@ def device_to_host(t, stream=None):
     if st != 0:
         raise DtbError(st, "Unable to transfert device to host")
     return out
+
+
+class BatchPlan:
+    """dtb_plan: a ragged batch of device tensors prepared once (descriptors, TMA tensor maps, scratch) and
+    captured in a CUDA graph; run() launches the graph, wait() returns the device status and counters."""
+
+    def __init__(self, imgs, masks, gammas, v=DEFAULT_V, dists=None, *, ctx=None):
+        n = len(imgs)
+        if dists is None:
+            dists = [_dist_like(t, None) for t in imgs]
+        self.imgs, self.masks, self.dists = list(imgs), list(masks), list(dists)  # keep the buffers alive
+        self.ctx = ctx if ctx is not None else _ctx_for(imgs[0], None)
+        vi = (DtbImage * n)(*[image_view(t, 3 if t.dim() == 3 else 1) for t in self.imgs])
+        vm = (DtbImage * n)(*[image_view(t, 1) for t in self.masks])
+        vd = (DtbImage * n)(*[image_view(t, 4) for t in self.dists])
+        g = (ctypes.c_float * n)(*[float(x) for x in gammas])
+        self._h = ctypes.c_void_p()
+        self.ctx.check(lib().dtb_plan_create(self.ctx.handle, n, vi, vm, vd, g, float(v), 0, ctypes.byref(self._h)))
+
+    def run(self, stream=None):
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        self.ctx.check(lib().dtb_plan_run(self._h, ctypes.c_void_p(_stream_ptr(stream))))
+
+    def wait(self, stream=None):
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        s = DtbStats()
+        self.ctx.check(lib().dtb_plan_wait(self._h, ctypes.c_void_p(_stream_ptr(stream)), ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in DtbStats._fields_}
+
+    def autotune(self, reps=3, stream=None):
+        if stream is None:
+            stream = torch.cuda.current_stream()
+        t = DtbTuning()
+        self.ctx.check(lib().dtb_plan_autotune(self._h, ctypes.c_void_p(_stream_ptr(stream)), int(reps), ctypes.byref(t)))
+        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent}
+
+    def close(self):
+        if self._h:
+            lib().dtb_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

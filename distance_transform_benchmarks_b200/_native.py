@@ -26,7 +26,8 @@ STATUS_NAMES = {
 DTB_SYMBOLS = [
     "dtb_abi_version", "dtb_status_string", "dtb_context_create", "dtb_context_destroy", "dtb_context_message",
     "dtb_last_stats", "dtb_sync", "dtb_gdt_ref", "dtb_gdt", "dtb_gdt_batch", "dtb_gdt_noalloc", "dtb_host_to_device",
-    "dtb_device_to_host",
+    "dtb_device_to_host", "dtb_context_set_tuning", "dtb_context_get_tuning", "dtb_plan_create", "dtb_plan_run",
+    "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy",
 ]
 
 
@@ -53,6 +54,10 @@ class DtbStats(ctypes.Structure):
         ("device_error_info", ctypes.c_uint32),
         ("kernel_ms", ctypes.c_double),
     ]
+
+
+class DtbTuning(ctypes.Structure):
+    _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32)]
 
 
 class DtbError(RuntimeError):
@@ -95,6 +100,20 @@ def lib():
         L.dtb_gdt.argtypes = [P, IMG, IMG, IMG, F, F, U32, P]
         L.dtb_gdt_batch.restype = I32
         L.dtb_gdt_batch.argtypes = [P, I32, IMG, IMG, IMG, ctypes.POINTER(F), F, U32, P]
+        L.dtb_context_set_tuning.restype = I32
+        L.dtb_context_set_tuning.argtypes = [P, ctypes.POINTER(DtbTuning)]
+        L.dtb_context_get_tuning.restype = I32
+        L.dtb_context_get_tuning.argtypes = [P, ctypes.POINTER(DtbTuning)]
+        L.dtb_plan_create.restype = I32
+        L.dtb_plan_create.argtypes = [P, I32, IMG, IMG, IMG, ctypes.POINTER(F), F, U32, ctypes.POINTER(P)]
+        L.dtb_plan_run.restype = I32
+        L.dtb_plan_run.argtypes = [P, P]
+        L.dtb_plan_wait.restype = I32
+        L.dtb_plan_wait.argtypes = [P, P, ctypes.POINTER(DtbStats)]
+        L.dtb_plan_autotune.restype = I32
+        L.dtb_plan_autotune.argtypes = [P, P, I32, ctypes.POINTER(DtbTuning)]
+        L.dtb_plan_destroy.restype = None
+        L.dtb_plan_destroy.argtypes = [P]
         L.dtb_gdt_noalloc.restype = I32
         L.dtb_gdt_noalloc.argtypes = [IMG, IMG, IMG, F, F, P]
         L.dtb_host_to_device.restype = I32

@@ -20,8 +20,8 @@
 #include <vector>
 
 #include "dtb.h"
-#include "dtb_kernels.cuh"
 #include "dtb_internal.h"
+#include "dtb_kernels.cuh"
 
 using namespace dtb;
 
@@ -140,56 +140,7 @@ __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__
 // ======================================================================================================
 // Host side
 // ======================================================================================================
-namespace {
-
-constexpr int PERSIST_WPC = 4;
-constexpr int PERSIST_MINB_REF = 2;
-// ns-mode persistent kernel variants: CTAs (of PERSIST_WPC warps) per SM, i.e. registers per thread
-// 255 / 168 / 128.  The choice is a tuning knob (dtb_context_set_tuning), default NS_VARIANT_DEFAULT.
-constexpr int NS_VARIANTS = 3;
-constexpr int NS_VARIANT_MINB[NS_VARIANTS] = {2, 3, 4};
-constexpr int NS_VARIANT_DEFAULT = 0;
-constexpr int ROUND_WPC = 4;
-constexpr size_t SMEM_SLOT = sizeof(WarpSmem);
-constexpr size_t PERSIST_SMEM = PERSIST_WPC * SMEM_SLOT + 128;
-constexpr size_t ROUND_SMEM = ROUND_WPC * SMEM_SLOT + 128;
-constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
-
-size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-uint32_t next_pow2(uint32_t x) {
-  uint32_t p = 1;
-  while (p < x) p <<= 1;
-  return p;
-}
-
-}  // namespace
-
-struct dtb_context_s {
-  int device = 0;
-  int num_sms = 0;
-  int persist_blocks_per_sm[2] = {0, 0};  // per weight mode (ns: of the selected variant)
-  const void* ns_fn[NS_VARIANTS] = {};
-  int ns_blocks_per_sm[NS_VARIANTS] = {};
-  int ns_variant = NS_VARIANT_DEFAULT;
-  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  void* dscratch = nullptr;
-  size_t dscratch_size = 0;
-  void* dstage = nullptr;
-  size_t dstage_size = 0;
-  std::vector<uint8_t> hstage;
-  std::string msg;
-  dtb_stats stats{};
-  // Asynchronous bookkeeping: header of the last enqueued run and the stream it ran on.
-  QueueHdr* last_hdr = nullptr;
-  uint64_t last_tiles = 0;
-  cudaStream_t last_stream = nullptr;
-  cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
-  bool timed = false;
-  bool async_pending = false;
-  std::mutex mu;
-};
-
-namespace {
+namespace dtb {
 
 dtb_status fail(dtb_context ctx, dtb_status s, const char* fmt, ...) {
   char buf[512];
@@ -206,13 +157,13 @@ dtb_status cuda_fail(dtb_context ctx, cudaError_t e, const char* what) {
   return fail(ctx, DTB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define DTB_CUDA(ctx, call)                                         \
-  do {                                                              \
-    cudaError_t e_ = (call);                                        \
-    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);      \
-  } while (0)
+static uint32_t next_pow2(uint32_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
 
-dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
+static dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
   if (*size >= need) return DTB_OK;
   if (*p) {
     cudaDeviceSynchronize();
@@ -222,13 +173,16 @@ dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
   }
   const size_t sz = align_up(need + need / 4, 1 << 20);
   cudaError_t e = cudaMalloc(p, sz);
-  if (e != cudaSuccess) { *p = nullptr; return cuda_fail(ctx, e, "cudaMalloc(scratch)"); }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(ctx, e, "cudaMalloc(scratch)");
+  }
   *size = sz;
   return DTB_OK;
 }
 
-bool encode_u8_2d(dtb_context ctx, CUtensorMap* out, const void* base, uint64_t row_bytes, uint64_t rows, uint64_t pitch,
-                  uint32_t box_w, uint32_t box_h) {
+static bool encode_u8_2d(dtb_context ctx, CUtensorMap* out, const void* base, uint64_t row_bytes, uint64_t rows,
+                         uint64_t pitch, uint32_t box_w, uint32_t box_h) {
   cuuint64_t dims[2] = {row_bytes, rows};
   cuuint64_t strides[1] = {pitch};
   cuuint32_t box[2] = {box_w, box_h};
@@ -238,13 +192,6 @@ bool encode_u8_2d(dtb_context ctx, CUtensorMap* out, const void* base, uint64_t 
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
-
-}  // namespace
-
-// ------------------------------------------------------------------------------------------------------
-// Jobs: one image each, already resolved to device memory with the alignment TMA needs.
-// ------------------------------------------------------------------------------------------------------
-namespace dtb {
 
 dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name, int elem_a, int elem_b) {
   if (!im) return fail(ctx, DTB_ERR_INVALID_ARG, "%s is NULL", name);
@@ -258,6 +205,190 @@ dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name,
     if ((int64_t)im->pitch < (int64_t)im->width * im->elem_size)
       return fail(ctx, DTB_ERR_INVALID_ARG, "%s: pitch %d < width * elem_size", name, im->pitch);
   }
+  return DTB_OK;
+}
+
+dtb_status check_triplet(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                         bool allow_rgb) {
+  dtb_status s;
+  if ((s = validate_view(ctx, img, "img", 1, allow_rgb ? 3 : 1)) != DTB_OK) return s;
+  if ((s = validate_view(ctx, mask, "mask", 1, 1)) != DTB_OK) return s;
+  if ((s = validate_view(ctx, dist, "dist", 4, 4)) != DTB_OK) return s;
+  if (img->width != mask->width || img->height != mask->height || img->width != dist->width || img->height != dist->height)
+    return fail(ctx, DTB_ERR_INVALID_ARG, "img, mask and dist must have the same size");
+  return DTB_OK;
+}
+
+dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* total) {
+  uint64_t t = 0;
+  for (const Job& j : jobs) t += (uint64_t)j.tiles_x() * j.tiles_y();
+  if (t >= (1ull << 31) || jobs.size() >= (1u << 23))
+    return fail(ctx, DTB_ERR_CAPACITY, "too many tiles (%llu) or images (%zu)", (unsigned long long)t, jobs.size());
+  *total = (uint32_t)t;
+  return DTB_OK;
+}
+
+uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t) {
+  const int bps = mode == MODE_NS ? ctx->ns_blocks_per_sm[t.variant] : ctx->ref_blocks_per_sm;
+  const uint32_t ctas = std::max<uint32_t>(1u, (uint32_t)(ctx->num_sms * bps) * (uint32_t)t.grid_percent / 100u);
+  return ctas * PERSIST_WPC;
+}
+
+ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds) {
+  ScratchLayout L;
+  L.n = n;
+  L.total = total;
+  L.cap = next_pow2(2u * (total + workers + 64u));
+  size_t off = 0;
+  L.o_hdr = off;    off = align_up(off + sizeof(QueueHdr), 256);
+  L.o_states = off; off = align_up(off + 4ull * std::max<uint32_t>(total, 1), 256);
+  L.o_ring = off;   off = align_up(off + 4ull * L.cap, 256);
+  L.o_desc = off;   off = align_up(off + sizeof(ImgDesc) * (size_t)std::max(n, 1), 256);
+  L.o_tmap = off;   off = align_up(off + sizeof(CUtensorMap) * 2 * (size_t)std::max(n, 1), 256);
+  L.o_base = off;   off = align_up(off + 4ull * (n + 1), 256);
+  L.o_act = off;    off = align_up(off + (rounds ? 2ull * std::max<uint32_t>(total, 1) : 0), 256);
+  L.o_chg = off;    off = align_up(off + 4, 256);
+  L.bytes = off;
+  return L;
+}
+
+dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const ScratchLayout& L, std::vector<uint8_t>& out) {
+  const int n = (int)jobs.size();
+  out.assign(L.o_act - L.o_desc, 0);
+  ImgDesc* hdesc = reinterpret_cast<ImgDesc*>(out.data());
+  CUtensorMap* htm = reinterpret_cast<CUtensorMap*>(out.data() + (L.o_tmap - L.o_desc));
+  uint32_t* hbase = reinterpret_cast<uint32_t*>(out.data() + (L.o_base - L.o_desc));
+  uint32_t base = 0;
+  for (int i = 0; i < n; ++i) {
+    const Job& j = jobs[i];
+    ImgDesc& d = hdesc[i];
+    d.img = j.img;
+    d.mask = j.mask;
+    d.dist = j.dist;
+    d.img_pitch = j.img_pitch;
+    d.mask_pitch = j.mask_pitch;
+    d.dist_pitch = j.dist_pitch;
+    d.width = j.width;
+    d.height = j.height;
+    d.channels = j.channels;
+    d.tiles_x = j.tiles_x();
+    d.tiles_y = j.tiles_y();
+    d.tile_base = base;
+    d.g2 = j.g2;
+    d.v = j.v;
+    d.l_eucl = j.l_eucl;
+    d.l_grad = j.l_grad;
+    d.mode = j.mode;
+    d.ref_fma = j.ref_fma;
+    hbase[i] = base;
+    base += (uint32_t)(d.tiles_x * d.tiles_y);
+    if (j.width > 0 && j.height > 0) {
+      const uint32_t bw = j.channels == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY;
+      if (!encode_u8_2d(ctx, &htm[2 * i], j.img, (uint64_t)j.width * j.channels, (uint64_t)j.height, (uint64_t)j.img_pitch,
+                        bw, IMG_BOX_ROWS))
+        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the image layout", i);
+      if (!encode_u8_2d(ctx, &htm[2 * i + 1], j.mask, (uint64_t)j.width, (uint64_t)j.height, (uint64_t)j.mask_pitch, TILE,
+                        TILE))
+        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the mask layout", i);
+    }
+  }
+  hbase[n] = base;
+  return DTB_OK;
+}
+
+uint64_t tuning_key(int n, uint32_t total) {
+  return ((uint64_t)next_pow2((uint32_t)std::max(n, 1)) << 32) | next_pow2(std::max<uint32_t>(total, 1));
+}
+
+static Queue make_queue(uint8_t* dbase, const ScratchLayout& L) {
+  const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * L.total + (1ull << 20));
+  // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
+  // this cap, which only turns a scheduling bug into an error instead of an endless run.
+  return Queue{reinterpret_cast<QueueHdr*>(dbase + L.o_hdr), reinterpret_cast<uint32_t*>(dbase + L.o_ring), L.cap - 1,
+               DEFAULT_TIMEOUT_NS, (uint32_t)cap_visits, L.total};
+}
+
+dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
+                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1) {
+  Queue q = make_queue(dbase, L);
+  const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + L.o_desc);
+  const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
+  const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
+  uint32_t* states = reinterpret_cast<uint32_t*>(dbase + L.o_states);
+  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_hdr, 0, sizeof(QueueHdr), stream));
+  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_ring, 0, 4ull * L.cap, stream));
+  if (L.total == 0) return DTB_OK;
+  const int n = L.n;
+  const uint32_t total = L.total;
+  const uint32_t scan_blocks = std::min<uint32_t>((total + 3) / 4, (uint32_t)ctx->num_sms * 16);
+  ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, nullptr, 0);
+  DTB_CUDA(ctx, cudaGetLastError());
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(resident_workers(ctx, mode, t) / PERSIST_WPC);
+  cfg.blockDim = dim3(PERSIST_WPC * 32);
+  cfg.dynamicSmemBytes = PERSIST_SMEM;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (ev0) DTB_CUDA(ctx, cudaEventRecord(ev0, stream));
+  void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
+  const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant] : (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
+  DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, fn, args));
+  if (ev1) DTB_CUDA(ctx, cudaEventRecord(ev1, stream));
+  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states);
+  DTB_CUDA(ctx, cudaGetLastError());
+  return DTB_OK;
+}
+
+// Host-driven rounds (the plain per-image path).  Synchronises once per round, like the reference's
+// blocks variant (generalised_distance_transform_blocks.cu:156-163).
+static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, cudaStream_t stream,
+                             uint64_t* nrounds) {
+  Queue q = make_queue(dbase, L);
+  const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + L.o_desc);
+  const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
+  const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
+  uint32_t* states = reinterpret_cast<uint32_t*>(dbase + L.o_states);
+  QueueHdr* hdr = reinterpret_cast<QueueHdr*>(dbase + L.o_hdr);
+  const uint32_t total = L.total;
+  uint8_t* act0 = dbase + L.o_act;
+  uint8_t* act1 = dbase + L.o_act + total;
+  uint32_t* changed = reinterpret_cast<uint32_t*>(dbase + L.o_chg);
+  DTB_CUDA(ctx, cudaMemsetAsync(hdr, 0, sizeof(QueueHdr), stream));
+  *nrounds = 0;
+  if (total == 0) return DTB_OK;
+  const uint32_t scan_blocks = std::min<uint32_t>((total + 3) / 4, (uint32_t)ctx->num_sms * 16);
+  DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
+  ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, L.n, total, states, q, act0, 0);
+  DTB_CUDA(ctx, cudaGetLastError());
+  uint8_t* cur = act0;
+  uint8_t* nxt = act1;
+  uint32_t hchanged = 1;
+  while (hchanged) {
+    DTB_CUDA(ctx, cudaMemsetAsync(nxt, 0, total, stream));
+    DTB_CUDA(ctx, cudaMemsetAsync(changed, 0, 4, stream));
+    const uint32_t blocks = (total + ROUND_WPC - 1) / ROUND_WPC;
+    if (mode == MODE_NS)
+      ggdt_round<MODE_NS, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
+    else
+      ggdt_round<MODE_REF, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
+    DTB_CUDA(ctx, cudaGetLastError());
+    uint32_t err_prog[2] = {0, 0};
+    DTB_CUDA(ctx, cudaMemcpyAsync(&hchanged, changed, 4, cudaMemcpyDeviceToHost, stream));
+    DTB_CUDA(ctx, cudaMemcpyAsync(&err_prog[0], &hdr->error.v, 4, cudaMemcpyDeviceToHost, stream));
+    DTB_CUDA(ctx, cudaMemcpyAsync(&err_prog[1], &hdr->progress.v, 4, cudaMemcpyDeviceToHost, stream));
+    DTB_CUDA(ctx, cudaStreamSynchronize(stream));
+    std::swap(cur, nxt);
+    ++*nrounds;
+    if (err_prog[0]) break;
+    if (err_prog[1] > q.max_visits)
+      return fail(ctx, DTB_ERR_DEVICE, "visit limit exceeded after %llu rounds", (unsigned long long)*nrounds);
+  }
+  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, L.n, total, states);
+  DTB_CUDA(ctx, cudaGetLastError());
   return DTB_OK;
 }
 
@@ -284,9 +415,7 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   std::vector<Job> jobs = jobs_in;
 
   // Serialise with a previous asynchronous call on another stream (the scratch is shared).
-  if (ctx->async_pending && ctx->last_stream != stream) {
-    DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
-  }
+  if (ctx->async_pending && ctx->last_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
 
   // ---- staging of inputs / outputs that are on the host or not aligned for TMA ----
   std::vector<Staged> staged;
@@ -296,8 +425,7 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
     const dtb_image* in3[3] = {imgs[i], masks[i], dists[i]};
     for (int k = 0; k < 3; ++k) {
       const dtb_image* u = in3[k];
-      const bool ok = (k < 2) ? tma_ok(u) : dist_ok(u);
-      if (ok) continue;
+      if ((k < 2) ? tma_ok(u) : dist_ok(u)) continue;
       const int64_t row = (int64_t)u->width * u->elem_size;
       const int64_t pitch = (int64_t)align_up((size_t)row, 128);
       staged.push_back({u, reinterpret_cast<uint8_t*>(stage_bytes), pitch, k < 2, k == 2});
@@ -316,9 +444,18 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   };
   for (int i = 0; i < n; ++i) {
     if (jobs[i].width == 0 || jobs[i].height == 0) continue;
-    if (const Staged* st = find_stage(imgs[i])) { jobs[i].img = st->dev; jobs[i].img_pitch = st->pitch; }
-    if (const Staged* st = find_stage(masks[i])) { jobs[i].mask = st->dev; jobs[i].mask_pitch = st->pitch; }
-    if (const Staged* st = find_stage(dists[i])) { jobs[i].dist = reinterpret_cast<float*>(st->dev); jobs[i].dist_pitch = st->pitch; }
+    if (const Staged* st = find_stage(imgs[i])) {
+      jobs[i].img = st->dev;
+      jobs[i].img_pitch = st->pitch;
+    }
+    if (const Staged* st = find_stage(masks[i])) {
+      jobs[i].mask = st->dev;
+      jobs[i].mask_pitch = st->pitch;
+    }
+    if (const Staged* st = find_stage(dists[i])) {
+      jobs[i].dist = reinterpret_cast<float*>(st->dev);
+      jobs[i].dist_pitch = st->pitch;
+    }
   }
   for (auto& st : staged) {
     if (!st.copy_in) continue;
@@ -328,167 +465,74 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
                                     (size_t)u->height, kind, stream));
   }
 
-  // ---- descriptor tables ----
-  uint64_t total64 = 0;
-  std::vector<uint32_t> base(n + 1);
-  for (int i = 0; i < n; ++i) {
-    base[i] = (uint32_t)total64;
-    total64 += (uint64_t)jobs[i].tiles_x() * jobs[i].tiles_y();
-  }
-  base[n] = (uint32_t)total64;
-  if (total64 >= (1ull << 31) || n >= (1 << 23)) return fail(ctx, DTB_ERR_CAPACITY, "too many tiles (%llu) or images", (unsigned long long)total64);
-  const uint32_t total = (uint32_t)total64;
+  // ---- descriptor tables and scratch ----
+  uint32_t total = 0;
+  dtb_status s = count_tiles(ctx, jobs, &total);
+  if (s != DTB_OK) return s;
   const bool rounds = (flags & DTB_FLAG_ROUNDS) != 0;
   const int mode = n > 0 ? jobs[0].mode : MODE_NS;
   for (int i = 1; i < n; ++i)
     if (jobs[i].mode != mode) return fail(ctx, DTB_ERR_INVALID_ARG, "one call covers images of one weight mode");
-
-  const uint32_t workers = (uint32_t)(ctx->num_sms * ctx->persist_blocks_per_sm[mode] * PERSIST_WPC);
-  const uint32_t cap = next_pow2(2u * (total + workers + 64u));
-
-  size_t off = 0;
-  const size_t o_hdr = off;   off = align_up(off + sizeof(QueueHdr), 256);
-  const size_t o_states = off; off = align_up(off + 4ull * std::max<uint32_t>(total, 1), 256);
-  const size_t o_ring = off;  off = align_up(off + 4ull * cap, 256);
-  const size_t o_desc = off;  off = align_up(off + sizeof(ImgDesc) * (size_t)std::max(n, 1), 256);
-  const size_t o_tmap = off;  off = align_up(off + sizeof(CUtensorMap) * 2 * (size_t)std::max(n, 1), 256);
-  const size_t o_base = off;  off = align_up(off + 4ull * (n + 1), 256);
-  const size_t o_act = off;   off = align_up(off + (rounds ? 2ull * std::max<uint32_t>(total, 1) : 0), 256);
-  const size_t o_chg = off;   off = align_up(off + 4, 256);
-  dtb_status s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, off);
-  if (s != DTB_OK) return s;
+  LaunchTuning tuning = ctx->tuning;
+  auto it = ctx->tuned.find(tuning_key(n, total));
+  if (it != ctx->tuned.end()) tuning = it->second;
+  const ScratchLayout L = layout_for(n, total, resident_workers(ctx, mode, tuning), rounds);
+  if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, L.bytes)) != DTB_OK) return s;
   uint8_t* dbase = reinterpret_cast<uint8_t*>(ctx->dscratch);
+  if ((s = build_tables(ctx, jobs, L, ctx->hstage)) != DTB_OK) return s;
+  DTB_CUDA(ctx, cudaMemcpyAsync(dbase + L.o_desc, ctx->hstage.data(), ctx->hstage.size(), cudaMemcpyHostToDevice, stream));
 
-  // Host image of [desc | tmaps | tile_base].
-  const size_t tbl_bytes = o_act - o_desc;
-  ctx->hstage.assign(tbl_bytes, 0);
-  ImgDesc* hdesc = reinterpret_cast<ImgDesc*>(ctx->hstage.data());
-  CUtensorMap* htm = reinterpret_cast<CUtensorMap*>(ctx->hstage.data() + (o_tmap - o_desc));
-  uint32_t* hbase = reinterpret_cast<uint32_t*>(ctx->hstage.data() + (o_base - o_desc));
-  for (int i = 0; i < n; ++i) {
-    const Job& j = jobs[i];
-    ImgDesc& d = hdesc[i];
-    d.img = j.img; d.mask = j.mask; d.dist = j.dist;
-    d.img_pitch = j.img_pitch; d.mask_pitch = j.mask_pitch; d.dist_pitch = j.dist_pitch;
-    d.width = j.width; d.height = j.height; d.channels = j.channels;
-    d.tiles_x = j.tiles_x(); d.tiles_y = j.tiles_y();
-    d.tile_base = base[i];
-    d.g2 = j.g2; d.v = j.v; d.l_eucl = j.l_eucl; d.l_grad = j.l_grad;
-    d.mode = j.mode; d.ref_fma = j.ref_fma;
-    hbase[i] = base[i];
-    if (j.width > 0 && j.height > 0) {
-      const uint32_t bw = j.channels == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY;
-      if (!encode_u8_2d(ctx, &htm[2 * i], j.img, (uint64_t)j.width * j.channels, (uint64_t)j.height, (uint64_t)j.img_pitch, bw,
-                        IMG_BOX_ROWS))
-        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the image layout", i);
-      if (!encode_u8_2d(ctx, &htm[2 * i + 1], j.mask, (uint64_t)j.width, (uint64_t)j.height, (uint64_t)j.mask_pitch, TILE, TILE))
-        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the mask layout", i);
-    }
-  }
-  hbase[n] = base[n];
-
-  QueueHdr* hdr = reinterpret_cast<QueueHdr*>(dbase + o_hdr);
-  uint32_t* states = reinterpret_cast<uint32_t*>(dbase + o_states);
-  uint32_t* ring = reinterpret_cast<uint32_t*>(dbase + o_ring);
-  const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + o_desc);
-  const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + o_tmap);
-  const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + o_base);
-  uint8_t* act0 = dbase + o_act;
-  uint8_t* act1 = dbase + o_act + total;
-  uint32_t* changed = reinterpret_cast<uint32_t*>(dbase + o_chg);
-
-  DTB_CUDA(ctx, cudaMemcpyAsync(dbase + o_desc, ctx->hstage.data(), tbl_bytes, cudaMemcpyHostToDevice, stream));
-  DTB_CUDA(ctx, cudaMemsetAsync(hdr, 0, sizeof(QueueHdr), stream));
-  DTB_CUDA(ctx, cudaMemsetAsync(ring, 0, 4ull * cap, stream));
-
-  // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
-  // this cap, which only turns a scheduling bug into an error instead of an endless run.
-  const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * total + (1ull << 20));
-  Queue q{hdr, ring, cap - 1, DEFAULT_TIMEOUT_NS, (uint32_t)cap_visits, total};
   uint64_t nrounds = 1;
-
-  if (total > 0) {
-    const uint32_t scan_blocks = std::min<uint32_t>((total + 3) / 4, (uint32_t)ctx->num_sms * 16);
-    if (!rounds) {
-      ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, nullptr, 0);
-      DTB_CUDA(ctx, cudaGetLastError());
-      cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3((unsigned)(ctx->num_sms * ctx->persist_blocks_per_sm[mode]));
-      cfg.blockDim = dim3(PERSIST_WPC * 32);
-      cfg.dynamicSmemBytes = PERSIST_SMEM;
-      cfg.stream = stream;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeCooperative;
-      attr[0].val.cooperative = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[0], stream));
-      if (mode == MODE_NS) {
-        void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
-        DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->ns_fn[ctx->ns_variant], args));
-      } else {
-        DTB_CUDA(ctx, cudaLaunchKernelEx(&cfg, ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB_REF>, ddesc, dtm, states, q));
-      }
-      if (flags & DTB_FLAG_TIMING) DTB_CUDA(ctx, cudaEventRecord(ctx->ev[1], stream));
-    } else {
-      DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
-      ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, act0, 0);
-      DTB_CUDA(ctx, cudaGetLastError());
-      uint8_t* cur = act0;
-      uint8_t* nxt = act1;
-      uint32_t hchanged = 1;
-      nrounds = 0;
-      while (hchanged) {
-        DTB_CUDA(ctx, cudaMemsetAsync(nxt, 0, total, stream));
-        DTB_CUDA(ctx, cudaMemsetAsync(changed, 0, 4, stream));
-        const uint32_t blocks = (total + ROUND_WPC - 1) / ROUND_WPC;
-        if (mode == MODE_NS)
-          ggdt_round<MODE_NS, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
-        else
-          ggdt_round<MODE_REF, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
-        DTB_CUDA(ctx, cudaGetLastError());
-        DTB_CUDA(ctx, cudaMemcpyAsync(&hchanged, changed, 4, cudaMemcpyDeviceToHost, stream));
-        DTB_CUDA(ctx, cudaStreamSynchronize(stream));
-        std::swap(cur, nxt);
-        ++nrounds;
-        uint32_t err_prog[2] = {0, 0};
-        DTB_CUDA(ctx, cudaMemcpy(&err_prog[0], &hdr->error.v, 4, cudaMemcpyDeviceToHost));
-        DTB_CUDA(ctx, cudaMemcpy(&err_prog[1], &hdr->progress.v, 4, cudaMemcpyDeviceToHost));
-        if (err_prog[0]) break;
-        if (err_prog[1] > cap_visits) return fail(ctx, DTB_ERR_DEVICE, "visit limit exceeded after %llu rounds", (unsigned long long)nrounds);
-      }
-    }
-    ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states);
-    DTB_CUDA(ctx, cudaGetLastError());
+  const bool timed = (flags & DTB_FLAG_TIMING) && !rounds && total > 0;
+  if (rounds) {
+    if ((s = run_rounds(ctx, dbase, L, mode, stream, &nrounds)) != DTB_OK) return s;
+  } else {
+    if ((s = enqueue_persistent(ctx, dbase, L, mode, tuning, stream, timed ? ctx->ev[0] : nullptr,
+                                timed ? ctx->ev[1] : nullptr)) != DTB_OK)
+      return s;
   }
 
   // ---- copy staged outputs back ----
-  bool host_out = false;
+  bool host_io = false;
   for (auto& st : staged) {
+    host_io |= st.user->memory_kind == DTB_CPU;
     if (!st.copy_out) continue;
     const dtb_image* u = st.user;
     const cudaMemcpyKind kind = u->memory_kind == DTB_CPU ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-    host_out |= u->memory_kind == DTB_CPU;
     DTB_CUDA(ctx, cudaMemcpy2DAsync(u->buffer, (size_t)u->pitch, st.dev, (size_t)st.pitch, (size_t)u->width * u->elem_size,
                                     (size_t)u->height, kind, stream));
   }
-  bool host_in = false;
-  for (auto& st : staged) host_in |= st.copy_in && st.user->memory_kind == DTB_CPU;
 
-  ctx->last_hdr = hdr;
-  ctx->last_tiles = total;
+  ctx->last_hdr = reinterpret_cast<QueueHdr*>(dbase + L.o_hdr);
   ctx->last_stream = stream;
   ctx->stats = dtb_stats{};
-  ctx->timed = (flags & DTB_FLAG_TIMING) && !rounds && total > 0;
   ctx->stats.tiles = total;
   ctx->stats.rounds = nrounds;
-  const bool async = (flags & DTB_FLAG_ASYNC) && !host_out && !host_in;
-  if (async) {
-    ctx->async_pending = true;
-    return DTB_OK;
-  }
+  ctx->timed = timed;
   ctx->async_pending = true;
+  if ((flags & DTB_FLAG_ASYNC) && !host_io) return DTB_OK;
   return dtb_sync(ctx, stream);
+}
+
+dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr_dev, dtb_stats* st) {
+  QueueHdr h;
+  DTB_CUDA(ctx, cudaMemcpy(&h, hdr_dev, sizeof(QueueHdr), cudaMemcpyDeviceToHost));
+  st->tile_visits = h.progress.v;
+  st->phases = h.phases.v;
+  st->activations = h.activations.v;
+  st->device_error = h.error.v;
+  st->device_error_info = h.err_info.v;
+  switch (h.error.v) {
+    case DERR_NONE: return DTB_OK;
+    case DERR_QUEUE_TIMEOUT:
+      return fail(ctx, DTB_ERR_TIMEOUT, "tile queue made no progress within the time limit (ticket %u)", h.err_info.v);
+    case DERR_TMA_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "TMA transfer of tile %u did not complete", h.err_info.v);
+    case DERR_PHASE_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile %u did not converge within %d phases", h.err_info.v, PHASE_LIMIT);
+    case DERR_RING_FULL: return fail(ctx, DTB_ERR_DEVICE, "queue ring slot stayed occupied (tile %u)", h.err_info.v);
+    case DERR_VISIT_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile visit limit exceeded (%u)", h.err_info.v);
+    case DERR_BAD_TILE: return fail(ctx, DTB_ERR_DEVICE, "internal error: activation of tile %u outside the call", h.err_info.v);
+    default: return fail(ctx, DTB_ERR_DEVICE, "device error %u", h.error.v);
+  }
 }
 
 }  // namespace dtb
@@ -539,34 +583,32 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
     delete ctx;
     return DTB_ERR_NO_DEVICE;
   }
-  ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[0]>;
-  ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[1]>;
-  ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_MINB[2]>;
-  for (int k = 0; k < NS_VARIANTS; ++k) {
-    if (cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], PERSIST_WPC * 32,
-                                                      PERSIST_SMEM) != cudaSuccess ||
-        ctx->ns_blocks_per_sm[k] < 1) {
-      delete ctx;
-      return DTB_ERR_NO_DEVICE;
-    }
+  ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[0]>;
+  ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[1]>;
+  ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[2]>;
+  const void* kref = (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
+  bool ok = true;
+  for (int k = 0; k < NS_VARIANTS && ok; ++k)
+    ok = cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], PERSIST_WPC * 32,
+                                                       PERSIST_SMEM) == cudaSuccess &&
+         ctx->ns_blocks_per_sm[k] >= 1;
+  ok = ok && cudaFuncSetAttribute(kref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
+       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ref_blocks_per_sm, kref, PERSIST_WPC * 32, PERSIST_SMEM) ==
+           cudaSuccess &&
+       ctx->ref_blocks_per_sm >= 1;
+  ok = ok &&
+       cudaFuncSetAttribute((const void*)ggdt_round<MODE_NS, ROUND_WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)ROUND_SMEM) == cudaSuccess &&
+       cudaFuncSetAttribute((const void*)ggdt_round<MODE_REF, ROUND_WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)ROUND_SMEM) == cudaSuccess;
+  if (!ok) {
+    delete ctx;
+    return DTB_ERR_NO_DEVICE;
   }
   if (const char* e = getenv("DTB_NS_VARIANT")) {
     const int k = atoi(e);
-    if (k >= 0 && k < NS_VARIANTS) ctx->ns_variant = k;
-  }
-  const void* kp[2] = {ctx->ns_fn[ctx->ns_variant],
-                        (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, PERSIST_MINB_REF>};
-  const void* kr[2] = {(const void*)ggdt_round<MODE_NS, ROUND_WPC>, (const void*)ggdt_round<MODE_REF, ROUND_WPC>};
-  for (int m = 0; m < 2; ++m) {
-    if (cudaFuncSetAttribute(kp[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(kr[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROUND_SMEM) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->persist_blocks_per_sm[m], kp[m], PERSIST_WPC * 32,
-                                                      PERSIST_SMEM) != cudaSuccess ||
-        ctx->persist_blocks_per_sm[m] < 1) {
-      delete ctx;
-      return DTB_ERR_NO_DEVICE;
-    }
+    if (k >= 0 && k < NS_VARIANTS) ctx->tuning.variant = k;
   }
   *out = ctx;
   return DTB_OK;
@@ -590,46 +632,45 @@ DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out) {
   return DTB_OK;
 }
 
+DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t) {
+  if (!ctx || !t) return DTB_ERR_INVALID_ARG;
+  int variant = ctx->tuning.variant;
+  if (t->ctas_per_sm != 0) {
+    variant = -1;
+    for (int k = 0; k < NS_VARIANTS; ++k)
+      if (NS_VARIANT_CTAS[k] == t->ctas_per_sm) variant = k;
+    if (variant < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "ctas_per_sm must be 2, 3 or 4");
+  }
+  const int pct = t->grid_percent == 0 ? 100 : t->grid_percent;
+  if (pct < 1 || pct > 100) return fail(ctx, DTB_ERR_INVALID_ARG, "grid_percent must be in [1, 100]");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->tuning.variant = variant;
+  ctx->tuning.grid_percent = pct;
+  ctx->tuned.clear();
+  return DTB_OK;
+}
+
+DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t) {
+  if (!ctx || !t) return DTB_ERR_INVALID_ARG;
+  t->ctas_per_sm = NS_VARIANT_CTAS[ctx->tuning.variant];
+  t->grid_percent = ctx->tuning.grid_percent;
+  return DTB_OK;
+}
+
 DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream) {
   if (!ctx) return DTB_ERR_INVALID_ARG;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   DTB_CUDA(ctx, cudaStreamSynchronize(st));
   if (!ctx->async_pending) return DTB_OK;
   ctx->async_pending = false;
-  QueueHdr h;
-  DTB_CUDA(ctx, cudaMemcpy(&h, ctx->last_hdr, sizeof(QueueHdr), cudaMemcpyDeviceToHost));
-  ctx->stats.tile_visits = h.progress.v;
-  ctx->stats.phases = h.phases.v;
-  ctx->stats.activations = h.activations.v;
-  ctx->stats.device_error = h.error.v;
-  ctx->stats.device_error_info = h.err_info.v;
+  const dtb_status s = read_device_status(ctx, ctx->last_hdr, &ctx->stats);
   if (ctx->timed) {
     float ms = 0.0f;
     DTB_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
     ctx->stats.kernel_ms = ms;
     ctx->timed = false;
   }
-  switch (h.error.v) {
-    case DERR_NONE: return DTB_OK;
-    case DERR_QUEUE_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "tile queue made no progress within the time limit (ticket %u)", h.err_info.v);
-    case DERR_TMA_TIMEOUT: return fail(ctx, DTB_ERR_TIMEOUT, "TMA transfer of tile %u did not complete", h.err_info.v);
-    case DERR_PHASE_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile %u did not converge within %d phases", h.err_info.v, PHASE_LIMIT);
-    case DERR_RING_FULL: return fail(ctx, DTB_ERR_DEVICE, "queue ring slot stayed occupied (tile %u)", h.err_info.v);
-    case DERR_VISIT_LIMIT: return fail(ctx, DTB_ERR_DEVICE, "tile visit limit exceeded (%u)", h.err_info.v);
-    case DERR_BAD_TILE: return fail(ctx, DTB_ERR_DEVICE, "internal error: activation of tile %u outside the call", h.err_info.v);
-    default: return fail(ctx, DTB_ERR_DEVICE, "device error %u", h.error.v);
-  }
-}
-
-static dtb_status check_pair(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
-                             bool allow_rgb) {
-  dtb_status s;
-  if ((s = validate_view(ctx, img, "img", 1, allow_rgb ? 3 : 1)) != DTB_OK) return s;
-  if ((s = validate_view(ctx, mask, "mask", 1, 1)) != DTB_OK) return s;
-  if ((s = validate_view(ctx, dist, "dist", 4, 4)) != DTB_OK) return s;
-  if (img->width != mask->width || img->height != mask->height || img->width != dist->width || img->height != dist->height)
-    return fail(ctx, DTB_ERR_INVALID_ARG, "img, mask and dist must have the same size");
-  return DTB_OK;
+  return s;
 }
 
 static bool valid_v(float v) { return v >= 0.0f; }  // also rejects NaN
@@ -639,7 +680,7 @@ DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_
   if (!ctx) return DTB_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->msg.clear();
-  dtb_status s = check_pair(ctx, img, mask, dist, false);
+  dtb_status s = check_triplet(ctx, img, mask, dist, false);
   if (s != DTB_OK) return s;
   if (!(lambda >= 0.0f && lambda <= 1.0f)) return fail(ctx, DTB_ERR_INVALID_ARG, "lambda must be in [0, 1]");
   if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
@@ -661,7 +702,7 @@ DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_imag
   if (!ctx) return DTB_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->msg.clear();
-  dtb_status s = check_pair(ctx, img, mask, dist, true);
+  dtb_status s = check_triplet(ctx, img, mask, dist, true);
   if (s != DTB_OK) return s;
   if (!(gamma >= 0.0f) || std::isinf(gamma)) return fail(ctx, DTB_ERR_INVALID_ARG, "gamma must be finite and >= 0");
   if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
@@ -687,7 +728,7 @@ DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* im
   std::vector<const dtb_image*> a(n), b(n), c(n);
   jobs.reserve(n);
   for (int i = 0; i < n; ++i) {
-    dtb_status s = check_pair(ctx, &imgs[i], &masks[i], &dists[i], true);
+    dtb_status s = check_triplet(ctx, &imgs[i], &masks[i], &dists[i], true);
     if (s != DTB_OK) return fail(ctx, s, "image %d: %s", i, ctx->msg.c_str());
     if (!(gammas[i] >= 0.0f) || std::isinf(gammas[i])) return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: bad gamma", i);
     Job j = Job::from(&imgs[i], &masks[i], &dists[i]);

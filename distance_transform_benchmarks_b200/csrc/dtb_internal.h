@@ -1,14 +1,31 @@
 // dtb_internal.h -- host-side types shared by the translation units of libdtb.
 #pragma once
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "dtb.h"
+#include "dtb_device.cuh"
 
 namespace dtb {
+
+constexpr int PERSIST_WPC = 4;   // warps per CTA of the persistent tile kernel
+constexpr int ROUND_WPC = 4;
+constexpr size_t PERSIST_SMEM = PERSIST_WPC * sizeof(WarpSmem) + 128;
+constexpr size_t ROUND_SMEM = ROUND_WPC * sizeof(WarpSmem) + 128;
+constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
+// ns-mode tile kernel variants: CTAs (of PERSIST_WPC warps) per SM, i.e. at most 255 / 168 / 128 registers.
+constexpr int NS_VARIANTS = 3;
+constexpr int NS_VARIANT_CTAS[NS_VARIANTS] = {2, 3, 4};
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // One image of a call, resolved to device memory.
 struct Job {
@@ -47,8 +64,78 @@ inline float gamma_to_g2(float gamma) {
   return g * g;
 }
 
+// Device scratch of one run: [queue header | tile states | ring | descriptors | tensor maps | tile prefix |
+// round flags | changed word], each part 256-byte aligned.
+struct ScratchLayout {
+  int n = 0;
+  uint32_t total = 0;  // tiles
+  uint32_t cap = 0;    // ring slots (power of two)
+  size_t o_hdr = 0, o_states = 0, o_ring = 0, o_desc = 0, o_tmap = 0, o_base = 0, o_act = 0, o_chg = 0, bytes = 0;
+};
+
+// Launch parameters of the tile kernel chosen for a run.
+struct LaunchTuning {
+  int variant = 0;        // ns-mode kernel variant (index into NS_VARIANT_CTAS)
+  int grid_percent = 100; // share of the co-resident CTAs that is launched
+};
+
+}  // namespace dtb
+
+struct dtb_context_s {
+  int device = 0;
+  int num_sms = 0;
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  const void* ns_fn[dtb::NS_VARIANTS] = {};
+  int ns_blocks_per_sm[dtb::NS_VARIANTS] = {};
+  int ref_blocks_per_sm = 0;
+  dtb::LaunchTuning tuning;                       // default tuning of this context
+  std::map<uint64_t, dtb::LaunchTuning> tuned;    // autotuner results by workload key
+  void* dscratch = nullptr;
+  size_t dscratch_size = 0;
+  void* dstage = nullptr;
+  size_t dstage_size = 0;
+  std::vector<uint8_t> hstage;
+  std::string msg;
+  dtb_stats stats{};
+  // Asynchronous bookkeeping: header of the last enqueued run and the stream it ran on.
+  dtb::QueueHdr* last_hdr = nullptr;
+  cudaStream_t last_stream = nullptr;
+  bool async_pending = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
+  bool timed = false;
+  std::mutex mu;
+};
+
+namespace dtb {
+
+dtb_status fail(dtb_context ctx, dtb_status s, const char* fmt, ...);
+dtb_status cuda_fail(dtb_context ctx, cudaError_t e, const char* what);
+#define DTB_CUDA(ctx, call)                                    \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+  } while (0)
+
 dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name, int elem_a, int elem_b);
+// Checks that img / mask / dist form one image of the given kinds (rgb allowed or not).
+dtb_status check_triplet(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist, bool allow_rgb);
+
+// Scratch layout for n images with `total` tiles, `workers` resident warps; `rounds` adds the round flags.
+ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds);
+// Host image of [descriptors | tensor maps | tile prefix] (bytes o_desc .. o_act of the layout).
+dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const ScratchLayout& L, std::vector<uint8_t>& out);
+// Total tiles of the jobs (error if beyond the 31-bit tile id space).
+dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* total);
+// Resident warps of the tile kernel of `mode` under `t`.
+uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t);
+// Enqueues queue reset, seed scan, the persistent tile kernel and finalize on `stream` (capturable).
+// ev0 / ev1 (optional) are recorded around the tile kernel.
+dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
+                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1);
 dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_image* const* imgs,
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
+// Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
+uint64_t tuning_key(int n, uint32_t total);
+dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);
 
 }  // namespace dtb

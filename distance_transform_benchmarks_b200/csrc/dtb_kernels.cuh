@@ -172,8 +172,8 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
 // One code path serves both layouts (the phase loop is small enough to stay in the instruction cache): the
 // weights live in shared memory as Wh / Wv (stride 33, conflict-free for a lane-per-row and a lane-per-column
 // read alike) and are loaded into registers for the phase's layout; the tile changes layout through B.
-// Element k of lane l of the current layout is at [k * sa + l * sb] of the plain row-major arrays
-// (column layout: sa = 33, sb = 1; row layout: sa = 1, sb = 33).
+// Element k of lane l is at [k * 33 + l] of the row-major arrays in the column layout, at [l * 33 + k] in the
+// row layout (immediate offsets from one base pointer per lane).
 // Returns the number of phases and activations through *nph / *nact.
 // ------------------------------------------------------------------------------------------------------
 template <class Sched>
@@ -275,27 +275,49 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   bool any = false, ran_col = false, ran_row = false, col = true;
   uint32_t nph = 0;
   for (;;) {
-    const int sa = col ? W_STRIDE : 1, sb = col ? 1 : W_STRIDE;
-    const float* Wc = col ? sm.Wv : sm.Wh;  // chain edges of the layout
-    const float* Wx = col ? sm.Wh : sm.Wv;  // cross edges
     float wc[TILE + 1], wx[TILE];
+    if (col) {  // element k of lane x: [k * 33 + x]
+      const float* pc = sm.Wv + lane;
+      const float* px = sm.Wh + lane;
 #pragma unroll
-    for (int k = 0; k <= TILE; ++k) wc[k] = Wc[k * sa + lane * sb];
+      for (int k = 0; k <= TILE; ++k) wc[k] = pc[k * W_STRIDE];
 #pragma unroll
-    for (int k = 0; k < TILE; ++k) wx[k] = Wx[k * sa + lane * sb];
+      for (int k = 0; k < TILE; ++k) wx[k] = px[k * W_STRIDE];
+    } else {    // element k of lane y: [y * 33 + k]
+      const float* pc = sm.Wh + lane * W_STRIDE;
+      const float* px = sm.Wv + lane * W_STRIDE;
+#pragma unroll
+      for (int k = 0; k <= TILE; ++k) wc[k] = pc[k];
+#pragma unroll
+      for (int k = 0; k < TILE; ++k) wx[k] = px[k];
+    }
     bool ch = sweep_phase(d, wc, wx, col ? top : lft, col ? bot : rgt);
     ch = __any_sync(~0u, ch);
     any |= ch;
     ran_col |= col;
     ran_row |= !col;
     ++nph;
+    const bool stop = (!ch && ran_col && ran_row) || nph >= (uint32_t)PHASE_LIMIT;
+    if (col) {
+      float* pb = B + lane;
 #pragma unroll
-    for (int k = 0; k < TILE; ++k) B[k * sa + lane * sb] = d[k];
-    __syncwarp();
-    if ((!ch && ran_col && ran_row) || nph >= (uint32_t)PHASE_LIMIT) break;
+      for (int k = 0; k < TILE; ++k) pb[k * W_STRIDE] = d[k];
+      __syncwarp();
+      if (stop) break;
+      const float* qb = B + lane * W_STRIDE;
+#pragma unroll
+      for (int k = 0; k < TILE; ++k) d[k] = qb[k];
+    } else {
+      float* pb = B + lane * W_STRIDE;
+#pragma unroll
+      for (int k = 0; k < TILE; ++k) pb[k] = d[k];
+      __syncwarp();
+      if (stop) break;
+      const float* qb = B + lane;
+#pragma unroll
+      for (int k = 0; k < TILE; ++k) d[k] = qb[k * W_STRIDE];
+    }
     col = !col;
-#pragma unroll
-    for (int k = 0; k < TILE; ++k) d[k] = B[k * sb + lane * sa];  // the other layout
     __syncwarp();
   }
   if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);

@@ -83,6 +83,17 @@ DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out);
 /* Waits for work enqueued with DTB_FLAG_ASYNC on `stream` and returns its device status. */
 DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
 
+/* Launch tuning of the ns-mode tile kernel (chosen by dtb_plan_autotune, or set by hand).
+ * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128; 0 = keep);
+ * grid_percent: share of the co-resident CTAs launched, 1..100 (fewer workers re-visit fewer tiles on
+ * narrow fronts; 0 = 100). */
+typedef struct dtb_tuning {
+  int32_t ctas_per_sm;
+  int32_t grid_percent;
+} dtb_tuning;
+DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t);
+DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t);
+
 /* Reference-weight GGDT (C8 neighbourhood, D(q) + (1-lambda)*{1, sqrt2} + lambda*|I(p)-I(q)|), gray input.
  * Replaces dt::generalised_distance_transform (generalised_distance_transform.hpp:7-8),
  * dt::generalised_distance_transform_blocks (:13-15) and dt::generalised_distance_transform_task (:21-23):
@@ -102,6 +113,23 @@ DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_imag
  * per call). */
 DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
                                  const dtb_image* dists, const float* gammas, float v, uint32_t flags, void* stream);
+
+/* Batch plans: a ragged ns-mode batch prepared once and run many times.  dtb_plan_create validates the views
+ * (device memory only: images and masks 16-byte aligned in buffer and pitch, distances 4-byte aligned), builds
+ * the image descriptors and TMA tensor maps, allocates the plan's own device scratch and captures one run
+ * (queue reset, seed scan, the cooperative persistent tile kernel, finalize) in a CUDA graph.  The buffers
+ * must stay allocated while the plan lives; their contents may change between runs.  dtb_plan_run launches
+ * the graph on `stream` and returns; dtb_plan_wait waits for it and returns the device status and counters
+ * (flags: reserved, pass 0).  dtb_plan_autotune times the tile-kernel launch variants on
+ * this batch (reps runs each), keeps the fastest in the plan and in the context's cache for batches of the
+ * same size class, and reports it.  No reference counterpart. */
+typedef struct dtb_plan_s* dtb_plan;
+DTB_API dtb_status dtb_plan_create(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
+                                   const dtb_image* dists, const float* gammas, float v, uint32_t flags, dtb_plan* out);
+DTB_API dtb_status dtb_plan_run(dtb_plan plan, void* stream);
+DTB_API dtb_status dtb_plan_wait(dtb_plan plan, void* stream, dtb_stats* stats);
+DTB_API dtb_status dtb_plan_autotune(dtb_plan plan, void* stream, int32_t reps, dtb_tuning* chosen);
+DTB_API void dtb_plan_destroy(dtb_plan plan);
 
 /* Allocation-free dtb_gdt for one image; no counterpart in the reference.
  * For callers that must not allocate device memory behind their own allocator: a host that owns all device

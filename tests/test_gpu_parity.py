@@ -222,3 +222,56 @@ def test_full_size_fixpoint(ctx, which):
     assert dmax < 2 ** 23, dmax
     assert va == 0 and vb == 0, (va, vb)
     assert ctx.stats()["device_error"] == 0
+
+
+def test_pitched_allocation_layout():
+    t = dtb.pitched_empty(5, 37, 3)
+    assert t.shape == (5, 37, 3) and t.stride() == (128, 3, 1)
+    f = dtb.pitched_empty(4, 33, 1, torch.float32)
+    assert f.stride() == (64, 1)  # 33 floats -> 256-byte rows
+
+
+def test_plan_rejects_unaligned_buffers(ctx):
+    img = torch.zeros((10, 37), dtype=torch.uint8, device="cuda")  # 37-byte pitch
+    with pytest.raises(dtb.DtbError):
+        dtb.BatchPlan([img], [img.clone()], [0.1], ctx=ctx)
+
+
+# ---------------------------------------------------------------------------------------------------
+# batch plans (CUDA graph) and the autotuner
+# ---------------------------------------------------------------------------------------------------
+def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
+    batch = wl.config3(seed=21, n=20, smin=24, smax=260)
+    imgs = [dtb.pitched_from(i) for i, _, _ in batch]
+    masks = [dtb.pitched_from(m) for _, m, _ in batch]
+    dists = [dtb.pitched_empty(i.shape[0], i.shape[1], 1, torch.float32).fill_(-1.0) for i, _, _ in batch]
+    plan = dtb.BatchPlan(imgs, masks, [g for _, _, g in batch], dists=dists, ctx=ctx)
+    refs = [orc.ggdt_ns(i, m, g) for i, m, g in batch]
+    for run in range(2):
+        for d in dists:
+            d.fill_(-1.0)
+        plan.run()
+        st = plan.wait()
+        assert st["device_error"] == 0 and st["tile_visits"] >= 1
+        for k, (d, ref) in enumerate(zip(dists, refs)):
+            assert_images_eq(d, ref, "plan run %d image %d" % (run, k))
+    chosen = plan.autotune(reps=1)
+    assert chosen["ctas_per_sm"] in (2, 3, 4) and 1 <= chosen["grid_percent"] <= 100
+    for d in dists:
+        d.fill_(-1.0)
+    plan.run()
+    plan.wait()
+    for k, (d, ref) in enumerate(zip(dists, refs)):
+        assert_images_eq(d, ref, "tuned plan image %d" % k)
+    plan.close()
+
+
+@pytest.mark.parametrize("ctas,pct", [(3, 100), (4, 50), (2, 25)])
+def test_every_tuning_gives_the_same_map(ctas, pct):
+    c = dtb.Context(0)
+    c.set_tuning(ctas_per_sm=ctas, grid_percent=pct)
+    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct}
+    img, mask, gamma = wl.config0(seed=9)
+    d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=c)
+    assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), "tuning %d/%d" % (ctas, pct))
+    c.close()
