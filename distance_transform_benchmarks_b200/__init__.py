@@ -53,13 +53,13 @@ class Context:
         self.check(lib().dtb_last_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in DtbStats._fields_}
 
-    def set_tuning(self, ctas_per_sm=0, grid_percent=0):
-        self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(DtbTuning(ctas_per_sm, grid_percent))))
+    def set_tuning(self, ctas_per_sm=0, grid_percent=0, host_chunk_kpx=0):
+        self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(DtbTuning(ctas_per_sm, grid_percent, host_chunk_kpx))))
 
     def get_tuning(self):
         t = DtbTuning()
         self.check(lib().dtb_context_get_tuning(self._h, ctypes.byref(t)))
-        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent}
+        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent, "host_chunk_kpx": t.host_chunk_kpx}
 
     def sync(self, stream=None):
         self.check(lib().dtb_sync(self._h, ctypes.c_void_p(_stream_ptr(stream))))

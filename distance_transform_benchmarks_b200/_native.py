@@ -57,7 +57,7 @@ class DtbStats(ctypes.Structure):
 
 
 class DtbTuning(ctypes.Structure):
-    _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32)]
+    _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32), ("host_chunk_kpx", ctypes.c_int32)]
 
 
 class DtbError(RuntimeError):

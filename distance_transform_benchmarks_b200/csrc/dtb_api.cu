@@ -163,7 +163,7 @@ static uint32_t next_pow2(uint32_t x) {
   return p;
 }
 
-static dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
+dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need) {
   if (*size >= need) return DTB_OK;
   if (*p) {
     cudaDeviceSynchronize();
@@ -416,6 +416,13 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
 
   // Serialise with a previous asynchronous call on another stream (the scratch is shared).
   if (ctx->async_pending && ctx->last_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
+  ctx->async_pending = false;
+
+  bool all_host = n > 0 && !(flags & DTB_FLAG_ROUNDS);
+  for (int i = 0; i < n && all_host; ++i)
+    all_host = jobs[i].mode == MODE_NS && imgs[i]->memory_kind == DTB_CPU && masks[i]->memory_kind == DTB_CPU &&
+               dists[i]->memory_kind == DTB_CPU;
+  if (all_host) return run_host_pipeline(ctx, jobs, imgs, masks, dists, stream);
 
   // ---- staging of inputs / outputs that are on the host or not aligned for TMA ----
   std::vector<Staged> staged;
@@ -621,6 +628,10 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (ctx->dstage) cudaFree(ctx->dstage);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->evpool)
+    if (e) cudaEventDestroy(e);
+  if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
+  if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
   delete ctx;
 }
 
@@ -643,9 +654,11 @@ DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t) 
   }
   const int pct = t->grid_percent == 0 ? 100 : t->grid_percent;
   if (pct < 1 || pct > 100) return fail(ctx, DTB_ERR_INVALID_ARG, "grid_percent must be in [1, 100]");
+  if (t->host_chunk_kpx < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "host_chunk_kpx must be >= 0");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->tuning.variant = variant;
   ctx->tuning.grid_percent = pct;
+  if (t->host_chunk_kpx > 0) ctx->host_chunk_px = (uint64_t)t->host_chunk_kpx * 1024ull;
   ctx->tuned.clear();
   return DTB_OK;
 }
@@ -654,6 +667,7 @@ DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t) {
   if (!ctx || !t) return DTB_ERR_INVALID_ARG;
   t->ctas_per_sm = NS_VARIANT_CTAS[ctx->tuning.variant];
   t->grid_percent = ctx->tuning.grid_percent;
+  t->host_chunk_kpx = (int32_t)(ctx->host_chunk_px / 1024ull);
   return DTB_OK;
 }
 

@@ -103,6 +103,10 @@ struct dtb_context_s {
   bool async_pending = false;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
   bool timed = false;
+  // Host-buffer pipeline: copy streams, events, chunk size in pixels.
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> evpool;
+  uint64_t host_chunk_px = 32ull << 20;
   std::mutex mu;
 };
 
@@ -134,6 +138,11 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
                               cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1);
 dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_image* const* imgs,
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
+// All images, masks and distances in host memory (ns-mode): chunked pipeline of 1-D host-to-device copies,
+// repitch, tile runs and 1-D device-to-host copies on overlapping streams.
+dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
+                             const dtb_image* const* masks, const dtb_image* const* dists, cudaStream_t stream);
+dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need);
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
 uint64_t tuning_key(int n, uint32_t total);
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);

@@ -183,6 +183,7 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
   if (chosen) {
     chosen->ctas_per_sm = NS_VARIANT_CTAS[best.variant];
     chosen->grid_percent = best.grid_percent;
+    chosen->host_chunk_kpx = (int32_t)(ctx->host_chunk_px / 1024ull);
   }
   return DTB_OK;
 }

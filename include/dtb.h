@@ -86,10 +86,13 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
 /* Launch tuning of the ns-mode tile kernel (chosen by dtb_plan_autotune, or set by hand).
  * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128; 0 = keep);
  * grid_percent: share of the co-resident CTAs launched, 1..100 (fewer workers re-visit fewer tiles on
- * narrow fronts; 0 = 100). */
+ * narrow fronts; 0 = 100); host_chunk_kpx: pixels (in units of 1024) per chunk of the pipeline that serves
+ * batches in host memory (host-to-device copies, tile runs and device-to-host copies of successive chunks
+ * overlap; 0 = keep, default 32768). */
 typedef struct dtb_tuning {
   int32_t ctas_per_sm;
   int32_t grid_percent;
+  int32_t host_chunk_kpx;
 } dtb_tuning;
 DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t);
 DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t);

@@ -200,6 +200,26 @@ def test_batch_vs_oracle_and_single(ctx):
         assert_images_eq(b, a.cpu().numpy(), "plain per-image vs batch %d" % k)
 
 
+def test_host_pipeline_many_chunks_padded_rows_and_empty_images():
+    c = dtb.Context(0)
+    c.set_tuning(host_chunk_kpx=24)  # ~24k pixels per chunk: many chunks, all overlapping
+    batch = wl.config3(seed=13, n=17, smin=20, smax=240)
+    imgs = [torch.from_numpy(i) for i, _, _ in batch]
+    masks = [torch.from_numpy(m) for _, m, _ in batch]
+    # a host image with padded rows (2-D copy path) and an empty image
+    big = torch.from_numpy(np.ascontiguousarray(np.pad(batch[0][0], ((0, 0), (0, 5)) + (((0, 0),) if batch[0][0].ndim == 3 else ()))))
+    imgs[0] = big[:, :batch[0][0].shape[1]]
+    imgs.append(torch.zeros((0, 7), dtype=torch.uint8))
+    masks.append(torch.zeros((0, 7), dtype=torch.uint8))
+    gammas = [g for _, _, g in batch] + [0.1]
+    dists = dtb.geodesic_distance_transform_batch(imgs, masks, gammas, ctx=c)
+    assert c.stats()["rounds"] > 3  # chunks
+    for k, (img, mask, g) in enumerate(batch):
+        assert_images_eq(dists[k], orc.ggdt_ns(img, mask, g), "pipeline image %d" % k)
+    assert dists[-1].shape == (0, 7)
+    c.close()
+
+
 def test_batch_host_buffers(ctx):
     batch = wl.config3(seed=12, n=6, smin=40, smax=200)
     dists = dtb.geodesic_distance_transform_batch([torch.from_numpy(i) for i, _, _ in batch],
@@ -270,7 +290,7 @@ def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
 def test_every_tuning_gives_the_same_map(ctas, pct):
     c = dtb.Context(0)
     c.set_tuning(ctas_per_sm=ctas, grid_percent=pct)
-    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct}
+    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 32768}
     img, mask, gamma = wl.config0(seed=9)
     d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=c)
     assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), "tuning %d/%d" % (ctas, pct))
