@@ -15,14 +15,15 @@ import threading
 import numpy as np
 import torch
 
-from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_FLAG_TIMING, DTB_GPU, DtbError,
-                      DtbImage, DtbStats, DtbTuning, lib)
+from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROUNDS, DTB_FLAG_TIMING, DTB_GPU,
+                      DTB_REQ_EDIT, DTB_REQ_IMAGE, DtbError, DtbImage, DtbServeCompletion, DtbServeConfig,
+                      DtbServeRequest, DtbServeStats, DtbStats, DtbTuning, lib)
 
 __all__ = [
     "Context", "DtbError", "default_context", "generalised_distance_transform",
     "generalised_distance_transform_blocks", "generalised_distance_transform_task", "geodesic_distance_transform",
     "geodesic_distance_transform_batch", "host_to_device", "device_to_host", "image_view", "DEFAULT_V", "BatchPlan",
-    "pitched_empty", "pitched_from",
+    "pitched_empty", "pitched_from", "Server",
 ]
 
 DEFAULT_V = 1e10  # reference default, generalised_distance_transform.hpp:8
@@ -295,6 +296,79 @@ class BatchPlan:
         if self._h:
             lib().dtb_plan_destroy(self._h)
             self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """dtb_server: continuous batching of new-image and seed-edit requests (see include/dtb.h).  Inputs and the
+    output map are host tensors (pinned memory copies fastest); they are kept alive here until the request's
+    completion has been polled."""
+
+    def __init__(self, hbm_budget_bytes, *, max_wave_requests=0, v=DEFAULT_V, ctx=None, device=0):
+        self.ctx = ctx if ctx is not None else default_context(device)
+        cfg = DtbServeConfig(int(hbm_budget_bytes), int(max_wave_requests), float(v))
+        self._h = ctypes.c_void_p()
+        st = lib().dtb_serve_create(self.ctx.handle, ctypes.byref(cfg), ctypes.byref(self._h))
+        if st != 0:
+            raise DtbError(st, "dtb_serve_create failed")
+        self._alive = {}
+
+    def _submit(self, req, keep):
+        rid = ctypes.c_int64()
+        st = lib().dtb_serve_submit(self._h, ctypes.byref(req), ctypes.byref(rid))
+        if st != 0:
+            raise DtbError(st, "dtb_serve_submit rejected the request")
+        self._alive[rid.value] = keep
+        return rid.value
+
+    def submit_image(self, image_id, img, mask, gamma, out):
+        img, mask = _as_tensor(img), _as_tensor(mask)
+        req = DtbServeRequest()
+        req.kind = DTB_REQ_IMAGE
+        req.image_id = int(image_id)
+        req.img = image_view(img, 3 if img.dim() == 3 else 1)
+        req.mask = image_view(mask, 1)
+        req.gamma = float(gamma)
+        req.out = image_view(out, 4)
+        return self._submit(req, (img, mask, out))
+
+    def submit_edit(self, image_id, disks, out):
+        arr = (ctypes.c_int32 * (3 * len(disks)))(*[int(v) for d in disks for v in d])
+        req = DtbServeRequest()
+        req.kind = DTB_REQ_EDIT
+        req.image_id = int(image_id)
+        req.n_disks = len(disks)
+        req.disks = ctypes.cast(arr, ctypes.POINTER(ctypes.c_int32))
+        req.out = image_view(out, 4)
+        return self._submit(req, (out,))
+
+    def poll(self, max_items=256, wait_ms=0):
+        buf = (DtbServeCompletion * max_items)()
+        k = lib().dtb_serve_poll(self._h, buf, max_items, int(wait_ms))
+        out = []
+        for c in buf[:k]:
+            self._alive.pop(c.request_id, None)
+            out.append({"request_id": c.request_id, "status": c.status, "latency_ms": c.latency_ms})
+        return out
+
+    def release(self, image_id):
+        return lib().dtb_serve_release(self._h, int(image_id))
+
+    def stats(self):
+        s = DtbServeStats()
+        lib().dtb_serve_get_stats(self._h, ctypes.byref(s))
+        return {f: getattr(s, f) for f, _ in DtbServeStats._fields_}
+
+    def close(self):
+        if self._h:
+            lib().dtb_serve_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._alive.clear()
 
     def __del__(self):
         try:

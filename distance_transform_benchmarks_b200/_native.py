@@ -27,8 +27,12 @@ DTB_SYMBOLS = [
     "dtb_abi_version", "dtb_status_string", "dtb_context_create", "dtb_context_destroy", "dtb_context_message",
     "dtb_last_stats", "dtb_sync", "dtb_gdt_ref", "dtb_gdt", "dtb_gdt_batch", "dtb_gdt_noalloc", "dtb_host_to_device",
     "dtb_device_to_host", "dtb_context_set_tuning", "dtb_context_get_tuning", "dtb_plan_create", "dtb_plan_run",
-    "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy",
+    "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy", "dtb_serve_create", "dtb_serve_submit", "dtb_serve_poll",
+    "dtb_serve_release", "dtb_serve_get_stats", "dtb_serve_destroy",
 ]
+
+DTB_REQ_IMAGE = 0
+DTB_REQ_EDIT = 1
 
 
 class DtbImage(ctypes.Structure):
@@ -58,6 +62,26 @@ class DtbStats(ctypes.Structure):
 
 class DtbTuning(ctypes.Structure):
     _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32), ("host_chunk_kpx", ctypes.c_int32)]
+
+
+class DtbServeConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_int32), ("v", ctypes.c_float)]
+
+
+class DtbServeRequest(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("image_id", ctypes.c_int64), ("img", DtbImage), ("mask", DtbImage),
+                ("gamma", ctypes.c_float), ("n_disks", ctypes.c_int32), ("disks", ctypes.POINTER(ctypes.c_int32)),
+                ("out", DtbImage)]
+
+
+class DtbServeCompletion(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_int64), ("status", ctypes.c_int32), ("latency_ms", ctypes.c_double)]
+
+
+class DtbServeStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "waves", "evictions", "pending",
+                                             "resident_images")] + \
+               [(n, ctypes.c_uint64) for n in ("resident_bytes", "tiles", "tile_visits")]
 
 
 class DtbError(RuntimeError):
@@ -114,6 +138,18 @@ def lib():
         L.dtb_plan_autotune.argtypes = [P, P, I32, ctypes.POINTER(DtbTuning)]
         L.dtb_plan_destroy.restype = None
         L.dtb_plan_destroy.argtypes = [P]
+        L.dtb_serve_create.restype = I32
+        L.dtb_serve_create.argtypes = [P, ctypes.POINTER(DtbServeConfig), ctypes.POINTER(P)]
+        L.dtb_serve_submit.restype = I32
+        L.dtb_serve_submit.argtypes = [P, ctypes.POINTER(DtbServeRequest), ctypes.POINTER(ctypes.c_int64)]
+        L.dtb_serve_poll.restype = I32
+        L.dtb_serve_poll.argtypes = [P, ctypes.POINTER(DtbServeCompletion), I32, I32]
+        L.dtb_serve_release.restype = I32
+        L.dtb_serve_release.argtypes = [P, ctypes.c_int64]
+        L.dtb_serve_get_stats.restype = I32
+        L.dtb_serve_get_stats.argtypes = [P, ctypes.POINTER(DtbServeStats)]
+        L.dtb_serve_destroy.restype = None
+        L.dtb_serve_destroy.argtypes = [P]
         L.dtb_gdt_noalloc.restype = I32
         L.dtb_gdt_noalloc.argtypes = [IMG, IMG, IMG, F, F, P]
         L.dtb_host_to_device.restype = I32

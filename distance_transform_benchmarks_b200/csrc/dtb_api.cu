@@ -300,7 +300,7 @@ uint64_t tuning_key(int n, uint32_t total) {
   return ((uint64_t)next_pow2((uint32_t)std::max(n, 1)) << 32) | next_pow2(std::max<uint32_t>(total, 1));
 }
 
-static Queue make_queue(uint8_t* dbase, const ScratchLayout& L) {
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L) {
   const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * L.total + (1ull << 20));
   // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
   // this cap, which only turns a scheduling bug into an error instead of an endless run.

@@ -16,16 +16,6 @@
 
 namespace dtb {
 
-// One image plane to move from packed rows (pitch = row_bytes) to rows of dst_pitch bytes.
-struct RepitchItem {
-  const uint8_t* src;
-  uint8_t* dst;
-  uint32_t row_bytes;
-  uint32_t rows;
-  uint32_t dst_pitch;
-  uint32_t row_base;  // prefix of rows over the items of the launch
-};
-
 // One warp per destination row; each lane assembles 4-byte words of the (128-byte aligned) destination row.
 __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restrict__ items, int n, uint32_t total_rows) {
   const int lane = threadIdx.x & 31;

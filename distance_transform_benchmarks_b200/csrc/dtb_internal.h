@@ -143,6 +143,20 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_ima
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
                              const dtb_image* const* masks, const dtb_image* const* dists, cudaStream_t stream);
 dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need);
+
+// Kernels shared across translation units (defined in dtb_api.cu / dtb_host_pipeline.cu).
+__global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
+                                                     int n, uint32_t total, const uint32_t* __restrict__ states);
+struct RepitchItem {
+  const uint8_t* src;
+  uint8_t* dst;
+  uint32_t row_bytes;
+  uint32_t rows;
+  uint32_t dst_pitch;
+  uint32_t row_base;  // prefix of rows over the items of the launch
+};
+__global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restrict__ items, int n, uint32_t total_rows);
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L);
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
 uint64_t tuning_key(int n, uint32_t total);
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);

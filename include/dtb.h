@@ -134,6 +134,48 @@ DTB_API dtb_status dtb_plan_wait(dtb_plan plan, void* stream, dtb_stats* stats);
 DTB_API dtb_status dtb_plan_autotune(dtb_plan plan, void* stream, int32_t reps, dtb_tuning* chosen);
 DTB_API void dtb_plan_destroy(dtb_plan plan);
 
+/* Serving engine: continuous batching of requests on one device.  A worker thread runs waves: each wave
+ * admits, in arrival order, the pending requests that fit the device-memory budget (evicting least recently
+ * used idle images) and runs all of them in one persistent launch over a shared tile queue; requests that
+ * arrive meanwhile join the next wave.  Images stay resident with their distance maps, so a seed edit
+ * warm-starts from the previous map (exact: added seeds only lower distances).  No reference counterpart.
+ * Request data (img, mask, out buffers) is host memory owned by the caller and must stay valid until the
+ * request's completion has been returned by dtb_serve_poll; the disk list is copied by dtb_serve_submit. */
+#define DTB_REQ_IMAGE 0  /* new image: img (gray / rgb8), mask, gamma; resident under image_id afterwards */
+#define DTB_REQ_EDIT 1   /* seed edit of the resident image image_id: n_disks disks (cx, cy, r) added */
+typedef struct dtb_serve_config {
+  uint64_t hbm_budget_bytes;  /* device memory reserved for resident images, masks and maps */
+  int32_t max_wave_requests;  /* at most this many requests per wave (0 = no limit) */
+  float v;                    /* value of unreached pixels (>= 0) */
+} dtb_serve_config;
+typedef struct dtb_serve_request {
+  int32_t kind;
+  int64_t image_id;
+  dtb_image img;
+  dtb_image mask;
+  float gamma;
+  int32_t n_disks;
+  const int32_t* disks;
+  dtb_image out;  /* host float map (elem_size 4) of the image's size: the result */
+} dtb_serve_request;
+typedef struct dtb_serve_completion {
+  int64_t request_id;
+  int32_t status;     /* dtb_status of the request */
+  double latency_ms;  /* from dtb_serve_submit to the result being in `out` */
+} dtb_serve_completion;
+typedef struct dtb_serve_stats {
+  int64_t submitted, completed, failed, waves, evictions, pending, resident_images;
+  uint64_t resident_bytes, tiles, tile_visits;
+} dtb_serve_stats;
+typedef struct dtb_server_s* dtb_server;
+DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg, dtb_server* out);
+DTB_API dtb_status dtb_serve_submit(dtb_server s, const dtb_serve_request* r, int64_t* request_id);
+/* Returns up to max completions, waiting up to wait_ms for the first one. */
+DTB_API int32_t dtb_serve_poll(dtb_server s, dtb_serve_completion* out, int32_t max, int32_t wait_ms);
+DTB_API dtb_status dtb_serve_release(dtb_server s, int64_t image_id);
+DTB_API dtb_status dtb_serve_get_stats(dtb_server s, dtb_serve_stats* out);
+DTB_API void dtb_serve_destroy(dtb_server s);
+
 /* Allocation-free dtb_gdt for one image; no counterpart in the reference.
  * For callers that must not allocate device memory behind their own allocator: a host that owns all device
  * memory through its own pool or budget, or a loop that cannot afford the device-wide synchronisation of

@@ -1,0 +1,115 @@
+"""GPU tests of the serving engine: every result is exact against the oracle, alone and in the mix.
+
+A new-image request must equal a cold run of its image and mask; a seed edit must equal a cold run with the
+union of the image's original seeds and every disk added to it so far (warm starts are exact because added
+seeds only lower distances).
+"""
+import time
+
+import numpy as np
+import pytest
+import torch
+
+import distance_transform_benchmarks_b200 as dtb
+from distance_transform_benchmarks_b200 import workloads as wl
+from oracle import oracle as orc
+from tests.helpers import assert_images_eq
+
+pytestmark = pytest.mark.gpu
+
+
+def _drain(srv, n, timeout=60.0):
+    got, t0 = {}, time.time()
+    while len(got) < n:
+        for c in srv.poll(wait_ms=50):
+            got[c["request_id"]] = c
+        assert time.time() - t0 < timeout, "serve requests did not complete"
+    return got
+
+
+def _images(seed, count, smin=40, smax=300):
+    return wl.config3(seed=seed, n=count, smin=smin, smax=smax)
+
+
+def _disks(rng, img, k):
+    h, w = img.shape[:2]
+    return [(int(rng.integers(0, w)), int(rng.integers(0, h)), 3) for _ in range(k)]
+
+
+def _mask_with(mask, disks):
+    h, w = mask.shape
+    return mask | wl.disks_mask(w, h, [(x, y) for x, y, _ in disks], [r for _, _, r in disks])
+
+
+def test_requests_in_the_mix_match_the_oracle_and_running_alone():
+    rng = np.random.default_rng(0)
+    batch = _images(31, 8)
+    srv = dtb.Server(256 << 20)
+    expected, outs = {}, {}
+    masks_now = {}
+    # all new images at once, then edits submitted while the first waves still run
+    for i, (img, mask, g) in enumerate(batch):
+        out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+        rid = srv.submit_image(100 + i, torch.from_numpy(img).pin_memory(), torch.from_numpy(mask).pin_memory(), g, out)
+        outs[rid] = out
+        expected[rid] = orc.ggdt_ns(img, mask, g)
+        masks_now[100 + i] = mask.copy()
+    for round_ in range(2):
+        for i in (1, 4, 6):
+            img, _, g = batch[i]
+            disks = _disks(rng, img, int(rng.integers(1, 4)))
+            masks_now[100 + i] = _mask_with(masks_now[100 + i], disks)
+            out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+            rid = srv.submit_edit(100 + i, disks, out)
+            outs[rid] = out
+            expected[rid] = orc.ggdt_ns(img, masks_now[100 + i], g)
+    got = _drain(srv, len(outs))
+    for rid, c in got.items():
+        assert c["status"] == 0, c
+        assert c["latency_ms"] > 0
+        assert_images_eq(outs[rid], expected[rid], "request %d" % rid)
+    st = srv.stats()
+    assert st["completed"] == len(outs) and st["failed"] == 0 and st["waves"] >= 1
+    srv.close()
+    # the same new image alone in its own server gives the same bits
+    img, mask, g = batch[4]
+    alone = dtb.Server(64 << 20)
+    out = torch.empty(img.shape[:2], dtype=torch.float32)
+    rid = alone.submit_image(1, torch.from_numpy(img), torch.from_numpy(mask), g, out)
+    assert _drain(alone, 1)[rid]["status"] == 0
+    first = [r for r in expected if np.array_equal(expected[r], orc.ggdt_ns(img, mask, g))][0]
+    assert_images_eq(out, outs[first].numpy(), "alone vs mixed")
+    alone.close()
+
+
+def test_budget_eviction_and_capacity():
+    batch = _images(32, 6, smin=200, smax=260)
+    def a128(x):
+        return -(-x // 128) * 128
+
+    def planes(img):  # device bytes of one resident image, as the engine lays them out
+        h, w = img.shape[:2]
+        c = 3 if img.ndim == 3 else 1
+        rb = w * c
+        return h * ((rb if rb % 16 == 0 else a128(rb)) + (w if w % 16 == 0 else a128(w)) + a128(4 * w)) + 3 * 256
+
+    per_image = max(planes(i) for i, _, _ in batch)
+    srv = dtb.Server(3 * per_image)
+    outs = {}
+    for i, (img, mask, g) in enumerate(batch):
+        out = torch.empty(img.shape[:2], dtype=torch.float32)
+        outs[srv.submit_image(i, torch.from_numpy(img), torch.from_numpy(mask), g, out)] = (out, img, mask, g)
+        _drain(srv, 1)  # one at a time: older images become evictable
+    for rid, (out, img, mask, g) in outs.items():
+        assert_images_eq(out, orc.ggdt_ns(img, mask, g), "evicting server %d" % rid)
+    st = srv.stats()
+    assert st["evictions"] >= 1
+    # an edit of an evicted image fails; an image larger than the whole budget fails
+    out = torch.empty(batch[0][0].shape[:2], dtype=torch.float32)
+    rid = srv.submit_edit(0, [(5, 5, 3)], out)
+    assert _drain(srv, 1)[rid]["status"] == 1
+    big = np.zeros((2048, 2048), np.uint8)
+    out = torch.empty((2048, 2048), dtype=torch.float32)
+    rid = srv.submit_image(99, torch.from_numpy(big), torch.from_numpy(big), 0.1, out)
+    assert _drain(srv, 1)[rid]["status"] == 7
+    srv.close()
