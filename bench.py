@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--seed", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=5000)
+    p.add_argument("--serve-rate", type=float, default=500.0, help="Poisson arrival rate (requests / s)")
+    p.add_argument("--no-serve", action="store_true")
     return p.parse_args()
 
 
@@ -187,6 +190,73 @@ def cpu_baseline(batch, seconds):
             "sample": "first %d images of the batch (%.1f Mpx), %.1f s" % (n, px / 1e6, dt)}
 
 
+SERVE_POOL = 48                 # distinct synthetic images behind the new-image requests
+SERVE_BUDGET = 120 << 30        # device-memory budget of the serving engine (bytes)
+
+
+def run_serve(args, dev):
+    """Serving workload: Poisson arrivals; 60 % new images (sides log-uniform in [256, 4096], gray blobs or rgb8
+    Voronoi, 1-8 seed disks), 40 % seed edits (1-3 disks of radius 3) of a resident image, warm-started from its
+    map.  Latency is measured by the engine from submit to the map being in host memory."""
+    import math
+    import distance_transform_benchmarks_b200 as dtb
+    from distance_transform_benchmarks_b200 import workloads as wl
+
+    rng = np.random.default_rng(4)
+    pool = []
+    for i in range(SERVE_POOL):
+        w = int(round(math.exp(rng.uniform(math.log(256), math.log(4096)))))
+        h = int(round(math.exp(rng.uniform(math.log(256), math.log(4096)))))
+        g = float(np.float32(rng.choice([0.01, 0.1, 1.0])))
+        img, mask, g = wl.make_image(("gray" if i % 2 == 0 else "rgb8", w, h, g, 1000 + i))
+        out = torch.empty((h, w), dtype=torch.float32).pin_memory()  # shared by the pool image's requests
+        pool.append((torch.from_numpy(img).pin_memory(), torch.from_numpy(mask).pin_memory(), g, out))
+    srv = dtb.Server(SERVE_BUDGET, device=dev)
+    n = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    kinds = rng.random(n) < 0.6
+    live = []          # (image id, pool index) of images created so far
+    pool_of = {}
+    lat, px, submitted = [], 0, 0
+    next_id = 0
+    t0 = time.perf_counter()
+    for k in range(n):
+        while time.perf_counter() - t0 < arrivals[k]:
+            for c in srv.poll(wait_ms=0):
+                lat.append(c["latency_ms"])
+            time.sleep(0.0002)
+        if kinds[k] or not live:
+            p = next_id % SERVE_POOL
+            img, mask, g, out = pool[p]
+            srv.submit_image(next_id, img, mask, g, out)
+            live.append(next_id)
+            pool_of[next_id] = p
+            next_id += 1
+        else:
+            iid = live[int(rng.integers(max(0, len(live) - 256), len(live)))]
+            img, _, _, out = pool[pool_of[iid]]
+            hh, ww = img.shape[:2]
+            disks = [(int(rng.integers(0, ww)), int(rng.integers(0, hh)), 3) for _ in range(int(rng.integers(1, 4)))]
+            srv.submit_edit(iid, disks, out)
+        px += int(img.shape[0]) * int(img.shape[1])
+        submitted += 1
+    while len(lat) < submitted:
+        for c in srv.poll(wait_ms=100):
+            lat.append(c["latency_ms"])
+        if time.perf_counter() - t0 > arrivals[-1] + 120:
+            break
+    elapsed = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat)
+    return {"requests": n, "rate_rps": args.serve_rate, "new_fraction": 0.6, "completed": int(st["completed"]),
+            "failed": int(st["failed"]), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "throughput_rps": len(lat) / elapsed, "mpx_s": px / 1e6 / elapsed,
+            "waves": int(st["waves"]), "requests_per_wave": len(lat) / max(1, st["waves"]),
+            "hbm_budget_gb": SERVE_BUDGET / 2 ** 30, "evictions": int(st["evictions"]),
+            "images": "sides log-U[256,4096], half gray blobs / half rgb8 Voronoi, %d distinct" % SERVE_POOL}
+
+
 def run_reference(args, dist):
     if dist.rank != 0:
         return
@@ -303,6 +373,7 @@ def run_ours(args, dist):
 
     # End to end through the C ABI with pinned host buffers.
     e2e = None
+    himgs = hmasks = hdists = None
     if not args.no_e2e:
         himgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
         hmasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]
@@ -341,6 +412,10 @@ def run_ours(args, dist):
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batch, CPU_SAMPLE_SECONDS)
+    serve = None
+    if not args.no_serve:
+        himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
+        serve = run_serve(args, dev)
 
     if dist.rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
@@ -359,7 +434,7 @@ def run_ours(args, dist):
                 "tile_stats": {"tiles": stats["tiles"], "visits_per_tile": stats["tile_visits"] / max(1, stats["tiles"]),
                                "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},
                 "gpu_launches": 3 * args.steps,
-                "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e}
+                "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serve": serve}
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()
