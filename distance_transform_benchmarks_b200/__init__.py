@@ -166,7 +166,7 @@ def _ctx_for(t, ctx):
     return default_context(dev)
 
 
-def _ref_call(img, mask, lam, v, dist, rounds, ctx, stream, fma):
+def _ref_call(img, mask, lam, v, dist, rounds, ctx, stream, fma, round_per_blocks=None):
     img, mask = _as_tensor(img), _as_tensor(mask)
     dist = _dist_like(img, dist)
     ctx = _ctx_for(img, ctx)
@@ -174,6 +174,15 @@ def _ref_call(img, mask, lam, v, dist, rounds, ctx, stream, fma):
         stream = torch.cuda.current_stream(img.device)
     vi, vm, vd = image_view(img, 1), image_view(mask, 1), image_view(dist, 4)
     flags = (DTB_FLAG_ROUNDS if rounds else 0) | (0 if fma else DTB_FLAG_REF_NO_FMA)
+    if round_per_blocks is not None:
+        tiles = ((img.shape[1] + 31) // 32) * ((img.shape[0] + 31) // 32)
+        if (round_per_blocks.dtype != torch.int32 or not round_per_blocks.is_contiguous()
+                or round_per_blocks.numel() != tiles):
+            raise ValueError("round_per_blocks must be a contiguous int32 tensor of %d tile counters" % tiles)
+        ctx.check(lib().dtb_gdt_ref_blocks(ctx.handle, ctypes.byref(vi), ctypes.byref(vm), ctypes.byref(vd), float(lam),
+                                           float(v), ctypes.c_void_p(round_per_blocks.data_ptr()), flags,
+                                           ctypes.c_void_p(_stream_ptr(stream))))
+        return dist
     ctx.check(lib().dtb_gdt_ref(ctx.handle, ctypes.byref(vi), ctypes.byref(vm), ctypes.byref(vd), float(lam), float(v),
                                 flags, ctypes.c_void_p(_stream_ptr(stream))))
     return dist
@@ -185,10 +194,12 @@ def generalised_distance_transform(img, mask, lam, v=DEFAULT_V, dist=None, *, ct
     return _ref_call(img, mask, lam, v, dist, False, ctx, stream, fma)
 
 
-def generalised_distance_transform_blocks(img, mask, lam, v=DEFAULT_V, dist=None, *, ctx=None, stream=None, fma=True):
+def generalised_distance_transform_blocks(img, mask, lam, v=DEFAULT_V, dist=None, round_per_blocks=None, *, ctx=None,
+                                          stream=None, fma=True):
     """dt::generalised_distance_transform_blocks (reference _blocks.cu:114-184): host-driven rounds over active
-    tiles.  Same result as the other two variants."""
-    return _ref_call(img, mask, lam, v, dist, True, ctx, stream, fma)
+    tiles.  Same result as the other two variants.  ``round_per_blocks``: optional int32 tensor (host or device)
+    of ceil(W/32)*ceil(H/32) counters, incremented once per round in which the tile was visited."""
+    return _ref_call(img, mask, lam, v, dist, True, ctx, stream, fma, round_per_blocks)
 
 
 def generalised_distance_transform_task(img, mask, lam, v=DEFAULT_V, dist=None, *, ctx=None, stream=None, fma=True):

@@ -1,8 +1,9 @@
 """Build recipes for the native libraries of the package (run by __graft_entry__.build()).
 
 * ``libdtb.so``        -- the CUDA kernels and the C ABI of include/dtb.h, compiled for sm_100a only.
-* ``libdtb_host.so``   -- host-only C++: synthetic workload generators and the serve engine front end.
-* ``libdt_b200.so``    -- the C++ ``namespace dt`` layer (include/dt/*.hpp) over the C ABI.
+* ``libdtb_host.so``   -- host-only C++: the seeded synthetic workload generators.
+
+The C++ ``namespace dt`` layer (include/dt/*.hpp) is header-only over libdtb.so.
 
 Everything is built in-tree next to this file; nothing is installed.
 """

@@ -116,6 +116,18 @@ __global__ void __launch_bounds__(WPC * 32)
   flush_stats(ws, q);
 }
 
+// dtb_gdt_ref_blocks: counts[t] += 1 for every tile visited in this round.
+__global__ void __launch_bounds__(256) ggdt_count_round(int32_t* __restrict__ counts, const uint8_t* __restrict__ active,
+                                                        uint32_t total) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) counts[t] += active[t] ? 1 : 0;
+}
+
+// counts[t] += add[t] (device-resident caller counters of dtb_gdt_ref_blocks).
+__global__ void __launch_bounds__(256) ggdt_add_counts(int32_t* __restrict__ counts, const int32_t* __restrict__ add,
+                                                       uint32_t total) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) counts[t] += add[t];
+}
+
 // Tiles never reached keep uninitialised memory: write v there.
 __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
                                                      int n, uint32_t total, const uint32_t* __restrict__ states) {
@@ -371,6 +383,11 @@ static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayou
     DTB_CUDA(ctx, cudaMemsetAsync(nxt, 0, total, stream));
     DTB_CUDA(ctx, cudaMemsetAsync(changed, 0, 4, stream));
     const uint32_t blocks = (total + ROUND_WPC - 1) / ROUND_WPC;
+    if (ctx->count_rounds) {
+      ggdt_count_round<<<std::min<uint32_t>((total + 255) / 256, (uint32_t)ctx->num_sms * 8), 256, 0, stream>>>(
+          ctx->dround_counts, cur, total);
+      DTB_CUDA(ctx, cudaGetLastError());
+    }
     if (mode == MODE_NS)
       ggdt_round<MODE_NS, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
     else
@@ -625,6 +642,7 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (!ctx) return;
   if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
   if (ctx->dscratch) cudaFree(ctx->dscratch);
+  if (ctx->dround_counts) cudaFree(ctx->dround_counts);
   if (ctx->dstage) cudaFree(ctx->dstage);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
@@ -711,6 +729,56 @@ DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_
   return run_jobs(ctx, {j}, a, b, c, flags, reinterpret_cast<cudaStream_t>(stream));
 }
 
+DTB_API dtb_status dtb_gdt_ref_blocks(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                                      float lambda, float v, int32_t* rounds_per_tile, uint32_t flags, void* stream) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->msg.clear();
+  dtb_status s = check_triplet(ctx, img, mask, dist, false);
+  if (s != DTB_OK) return s;
+  if (!(lambda >= 0.0f && lambda <= 1.0f)) return fail(ctx, DTB_ERR_INVALID_ARG, "lambda must be in [0, 1]");
+  if (!valid_v(v)) return fail(ctx, DTB_ERR_INVALID_ARG, "v must be >= 0");
+  DTB_CUDA(ctx, cudaSetDevice(ctx->device));
+  Job j = Job::from(img, mask, dist);
+  j.mode = MODE_REF;
+  j.v = v;
+  j.l_grad = lambda;
+  j.l_eucl = 1.0f - lambda;
+  j.ref_fma = (flags & DTB_FLAG_REF_NO_FMA) ? 0 : 1;
+  const dtb_image* a[1] = {img};
+  const dtb_image* b[1] = {mask};
+  const dtb_image* c[1] = {dist};
+  const uint32_t total = (uint32_t)j.tiles_x() * (uint32_t)j.tiles_y();
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const bool counting = rounds_per_tile != nullptr && total > 0;
+  if (counting) {
+    if ((s = grow(ctx, reinterpret_cast<void**>(&ctx->dround_counts), &ctx->dround_counts_size, total * sizeof(int32_t))) != DTB_OK)
+      return s;
+    DTB_CUDA(ctx, cudaMemsetAsync(ctx->dround_counts, 0, total * sizeof(int32_t), st));
+  }
+  ctx->count_rounds = counting;
+  s = run_jobs(ctx, {j}, a, b, c, (flags | DTB_FLAG_ROUNDS) & ~DTB_FLAG_ASYNC, st);
+  ctx->count_rounds = false;
+  if (s != DTB_OK || !counting) return s;
+  // Add this call's counters into the caller's (host or device memory).
+  cudaPointerAttributes pa{};
+  const bool on_device = cudaPointerGetAttributes(&pa, rounds_per_tile) == cudaSuccess &&
+                         (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+  cudaGetLastError();  // cudaPointerGetAttributes on plain host memory may leave an error behind on older drivers
+  if (on_device) {
+    ggdt_add_counts<<<std::min<uint32_t>((total + 255) / 256, (uint32_t)ctx->num_sms * 8), 256, 0, st>>>(
+        rounds_per_tile, ctx->dround_counts, total);
+    DTB_CUDA(ctx, cudaGetLastError());
+    DTB_CUDA(ctx, cudaStreamSynchronize(st));
+  } else {
+    std::vector<int32_t> h(total);
+    DTB_CUDA(ctx, cudaMemcpyAsync(h.data(), ctx->dround_counts, total * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    DTB_CUDA(ctx, cudaStreamSynchronize(st));
+    for (uint32_t t = 0; t < total; ++t) rounds_per_tile[t] += h[t];
+  }
+  return DTB_OK;
+}
+
 DTB_API dtb_status dtb_gdt(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist, float gamma,
                            float v, uint32_t flags, void* stream) {
   if (!ctx) return DTB_ERR_INVALID_ARG;
@@ -782,6 +850,45 @@ static dtb_status copy2d(const dtb_image* src, const dtb_image* dst, cudaMemcpyK
                                     (size_t)src->width * src->elem_size, (size_t)src->height, kind, st);
   if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(st);
   return e == cudaSuccess ? DTB_OK : DTB_ERR_CUDA;
+}
+
+DTB_API dtb_status dtb_image_alloc(int32_t width, int32_t height, int32_t elem_size, int32_t memory_kind, dtb_image* out) {
+  if (!out || width < 0 || height < 0 || elem_size <= 0 || (memory_kind != DTB_CPU && memory_kind != DTB_GPU))
+    return DTB_ERR_INVALID_ARG;
+  const size_t row = (size_t)width * (size_t)elem_size;
+  const size_t pitch = memory_kind == DTB_GPU ? align_up(std::max<size_t>(row, 1), 128) : row;
+  if (pitch > (size_t)INT32_MAX) return DTB_ERR_INVALID_ARG;
+  const size_t bytes = pitch * (size_t)height;
+  void* p = nullptr;
+  if (bytes > 0) {
+    if (memory_kind == DTB_GPU) {
+      const cudaError_t e = cudaMalloc(&p, bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (e == cudaErrorMemoryAllocation) return DTB_ERR_OUT_OF_MEMORY;
+        if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return DTB_ERR_NO_DEVICE;
+        return DTB_ERR_CUDA;
+      }
+    } else {
+      p = std::aligned_alloc(64, align_up(bytes, 64));
+      if (!p) return DTB_ERR_OUT_OF_MEMORY;
+    }
+  }
+  *out = dtb_image{p, width, height, (int32_t)pitch, elem_size, memory_kind};
+  return DTB_OK;
+}
+
+DTB_API dtb_status dtb_image_free(dtb_image* img) {
+  if (!img) return DTB_ERR_INVALID_ARG;
+  if (img->buffer) {
+    if (img->memory_kind == DTB_GPU) {
+      if (cudaFree(img->buffer) != cudaSuccess) return DTB_ERR_CUDA;
+    } else {
+      std::free(img->buffer);
+    }
+  }
+  img->buffer = nullptr;
+  return DTB_OK;
 }
 
 DTB_API dtb_status dtb_host_to_device(const dtb_image* src, const dtb_image* dst, void* stream) {

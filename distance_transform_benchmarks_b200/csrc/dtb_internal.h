@@ -107,6 +107,10 @@ struct dtb_context_s {
   cudaStream_t s_in = nullptr, s_out = nullptr;
   std::vector<cudaEvent_t> evpool;
   uint64_t host_chunk_px = 32ull << 20;
+  // dtb_gdt_ref_blocks: per-tile round counters of the running call (device scratch of `total` int32).
+  int32_t* dround_counts = nullptr;
+  size_t dround_counts_size = 0;
+  bool count_rounds = false;
   std::mutex mu;
 };
 

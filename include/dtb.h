@@ -105,6 +105,15 @@ DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t);
 DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
                                float lambda, float v, uint32_t flags, void* stream);
 
+/* dt::generalised_distance_transform_blocks with its round counters
+ * (generalised_distance_transform.hpp:13-15, _blocks.cu:114-165): ref-mode GGDT by host-driven rounds over
+ * active 32x32 tiles (DTB_FLAG_ROUNDS is implied).  rounds_per_tile, if not NULL, points to
+ * ceil(width/32) * ceil(height/32) int32 counters, tile (bx, by) at index by * ceil(width/32) + bx, in host or
+ * device memory; each is incremented once per round in which its tile was visited (the first round visits
+ * the tiles holding seeds, where the reference's first round visits every tile).  Same map as dtb_gdt_ref. */
+DTB_API dtb_status dtb_gdt_ref_blocks(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
+                                      float lambda, float v, int32_t* rounds_per_tile, uint32_t flags, void* stream);
+
 /* Geodesic GGDT with C4 connectivity and w(p,q) = sqrt(1 + gamma^2 * |I(p)-I(q)|^2); gray (elem_size 1)
  * or rgb8 (elem_size 3, |.| the Euclidean RGB difference).  Extends the reference entry point of
  * generalised_distance_transform.hpp:7-8 to the C4 neighbourhood (dt/include/dt/c4.hpp:9-27) and rgb8. */
@@ -189,6 +198,14 @@ DTB_API void dtb_serve_destroy(dtb_server s);
  * at zero; calls that overlap on the GPU (other threads or streams) race on it and must be serialised. */
 DTB_API dtb_status dtb_gdt_noalloc(const dtb_image* img, const dtb_image* mask, const dtb_image* dist, float gamma,
                                    float v, void* stream);
+
+/* Pitched image storage, reference dt::image2d<T> allocation (dt/include/dt/image2d.hpp:36-50,
+ * details/image2d_data_gpu.hpp:23-39).  DTB_GPU: device memory of the current device, pitch rounded up to
+ * 128 bytes (the alignment the tile kernel's bulk tensor copies read fastest); DTB_CPU: host memory, pitch =
+ * width * elem_size as in the reference.  Fills *out (buffer, width, height, pitch, elem_size, memory_kind).
+ * dtb_image_free releases it (NULL buffer: no-op) and clears out->buffer. */
+DTB_API dtb_status dtb_image_alloc(int32_t width, int32_t height, int32_t elem_size, int32_t memory_kind, dtb_image* out);
+DTB_API dtb_status dtb_image_free(dtb_image* img);
 
 /* Host <-> device copies of a pitched image, reference dt::host_to_device / dt::device_to_host
  * (dt/include/dt/transfert.hpp:13-15, dt/src/transfert.cpp:10-28).  Synchronous when stream is NULL. */

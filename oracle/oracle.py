@@ -13,7 +13,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_PASSES_PATH = os.path.join(HERE, "_ref", "libref_passes.so")
 _lib = None
+_ref_lib = None
 
 
 def build(force=False):
@@ -21,6 +23,53 @@ def build(force=False):
     if force or not os.path.exists(LIB_PATH) or os.path.getmtime(src) > os.path.getmtime(LIB_PATH):
         subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []), check=True)
     return LIB_PATH
+
+
+REF_TESTS = ("image_view", "image2d", "c4", "rgb8", "transfert", "distance_transform")
+
+
+def build_ref(ref_root, force=False):
+    """Builds, from the reference source tree at `ref_root`, into _ref/: the reference's tile-pass device
+    functions (libref_passes.so, see ref_passes_driver.cu) and the reference's own unit tests compiled against
+    include/dt and libdtb (test_<name>, see gtest_shim/).  libdtb must be built first.  Returns False if
+    `ref_root` is absent."""
+    if not os.path.isdir(os.path.join(ref_root, "dt", "src")):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "ref", "ref-tests", "REF_ROOT=" + ref_root] + (["-B"] if force else []),
+                   check=True)
+    return True
+
+
+def ref_test_binary(name):
+    """Path of the reference unit test `name` built by build_ref, or None if it was not built."""
+    p = os.path.join(HERE, "_ref", "test_" + name)
+    return p if os.path.exists(p) else None
+
+
+def ref_passes_available():
+    return os.path.exists(REF_PASSES_PATH)
+
+
+def ref_passes(imgs, masks, lam, v=1e10):
+    """The reference's compiled ref-mode arithmetic (dt/src/dt_block_passes.cuh:12-127) run to quiescence on the
+    GPU, for a stack of n images of at most 32x32 pixels (uint8 [n, h, w] image and seed mask).  Needs a GPU
+    and _ref/libref_passes.so."""
+    global _ref_lib
+    if _ref_lib is None:
+        L = ctypes.CDLL(REF_PASSES_PATH)
+        P, I, F = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        L.refp_gdt_tiles.restype = I
+        L.refp_gdt_tiles.argtypes = [P, P, P, I, I, I, F, F]
+        _ref_lib = L
+    imgs = _c(np.asarray(imgs, dtype=np.uint8))
+    masks = _c(np.asarray(masks, dtype=np.uint8))
+    n, h, w = imgs.shape
+    assert masks.shape == imgs.shape
+    out = np.empty((n, h, w), dtype=np.float32)
+    rc = _ref_lib.refp_gdt_tiles(imgs.ctypes.data, masks.ctypes.data, out.ctypes.data, n, w, h, float(lam), float(v))
+    if rc != 0:
+        raise RuntimeError("refp_gdt_tiles failed with code %d" % rc)
+    return out
 
 
 def lib():
