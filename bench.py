@@ -47,50 +47,15 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=5000)
     p.add_argument("--serve-rate", type=float, default=500.0, help="Poisson arrival rate (requests / s)")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-ref-mode", action="store_true")
+    p.add_argument("--ref-mpx", type=float, default=REF_STEP_MPX, help="reference arm: pixels per step (millions)")
     return p.parse_args()
 
 
 # ---------------------------------------------------------------------------------------------------------
 # distributed plumbing (timing only: the max of the step times over ranks)
 # ---------------------------------------------------------------------------------------------------------
-class Dist:
-    def __init__(self):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = False
-
-    def init(self, backend):
-        if self.world > 1:
-            import torch.distributed as td
-            td.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
-            self.pg = True
-
-    def barrier(self):
-        if self.pg:
-            import torch.distributed as td
-            td.barrier()
-
-    def max(self, x, device):
-        if not self.pg:
-            return x
-        import torch.distributed as td
-        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum(self, x, device):
-        if not self.pg:
-            return x
-        import torch.distributed as td
-        t = torch.tensor([float(x)], dtype=torch.float64, device=device)
-        td.all_reduce(t, op=td.ReduceOp.SUM)
-        return float(t.item())
-
-    def close(self):
-        if self.pg:
-            import torch.distributed as td
-            td.destroy_process_group()
+from distance_transform_benchmarks_b200.replicas import ReplicaGroup as Dist  # noqa: E402
 
 
 # ---------------------------------------------------------------------------------------------------------
@@ -194,6 +159,46 @@ SERVE_POOL = 48                 # distinct synthetic images behind the new-image
 SERVE_BUDGET = 120 << 30        # device-memory budget of the serving engine (bytes)
 
 
+# The reference's own benchmark (benchmarks/distance_transform.cpp): reference weight (C8, lambda blend) on
+# ~8.9 Mpx gray photographs, lambda in {0, 0.5, 1}, one call per image timed whole (allocation and setup
+# included).  Published throughput on its (unrecorded) GPU, Mpixel/s: raster 55.8 / 28.0 / 25.1, blocks
+# 375 / 324 / 323, task 613 / 555 / 560 for lambda 0 / 0.5 / 1.  The photographs are not available: a seeded
+# 3648 x 2432 (8.87 Mpx) gray blob image with 8 seed disks stands in for them.
+REF_MODE_W, REF_MODE_H = 3648, 2432
+REF_PUBLISHED = {"raster": [55.8, 28.0, 25.1], "blocks": [375.0, 324.0, 323.0], "task": [613.0, 555.0, 560.0]}
+
+
+def run_ref_mode(args, ctx, stream):
+    import distance_transform_benchmarks_b200 as dtb
+    from distance_transform_benchmarks_b200 import workloads as wl
+    img = wl.blobs_gray(args.seed + 77, REF_MODE_W, REF_MODE_H)
+    mask = wl.random_disks(np.random.default_rng(args.seed + 78), REF_MODE_W, REF_MODE_H, 8, 2, 6)
+    ti, tm = torch.from_numpy(img).cuda(), torch.from_numpy(mask).cuda()
+    px = REF_MODE_W * REF_MODE_H
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    variants = (("task", dtb.generalised_distance_transform_task), ("blocks", dtb.generalised_distance_transform_blocks))
+    for name, fn in variants:
+        vals = []
+        for lam in (0.0, 0.5, 1.0):
+            fn(ti, tm, lam, ctx=ctx, stream=stream)  # warm-up (scratch growth, module load)
+            reps = 3
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                fn(ti, tm, lam, ctx=ctx, stream=stream)  # allocating call, as the reference benchmark times it
+            e1.record(stream)
+            torch.cuda.synchronize()
+            vals.append(px / 1e6 / (e0.elapsed_time(e1) / reps / 1e3))
+        out[name] = vals
+    return {"image": "%dx%d gray blobs, 8 seed disks r 2-6 (stands in for the reference's ~8.9 Mpx photographs)"
+                     % (REF_MODE_W, REF_MODE_H),
+            "lambdas": [0.0, 0.5, 1.0], "mpx_s": out, "unit": UNIT,
+            "reference_published_mpx_s": REF_PUBLISHED,
+            "note": "whole call timed on the stream (allocation + setup + transform), inputs resident on the device; "
+                    "task = persistent tile queue (the raster variant returns the same map through the same path)"}
+
+
 def run_serve(args, dev):
     """Serving workload: Poisson arrivals; 60 % new images (sides log-uniform in [256, 4096], gray blobs or rgb8
     Voronoi, 1-8 seed disks), 40 % seed edits (1-3 disks of radius 3) of a resident image, warm-started from its
@@ -267,7 +272,7 @@ def run_reference(args, dist):
     for s in specs:
         sample.append(wl.make_image(s))
         px += s[1] * s[2]
-        if px >= REF_STEP_MPX * 1e6:
+        if px >= args.ref_mpx * 1e6:
             break
     for _ in range(args.warmup):
         for img, mask, g in sample[:4]:
@@ -300,7 +305,7 @@ def run_ours(args, dist):
     ctx = dtb.Context(dev)
     stream = torch.cuda.current_stream()
 
-    batch = wl.config3(seed=args.seed + 1000 * dist.rank, n=args.images)
+    batch = wl.config3(seed=dist.seed(args.seed), n=args.images)
     px = wl.pixels(batch)
     alg_bytes = sum(img.shape[0] * img.shape[1] * wl.bytes_per_pixel(img) for img, _, _ in batch)
     imgs = [dtb.pitched_from(i) for i, _, _ in batch]
@@ -412,6 +417,7 @@ def run_ours(args, dist):
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batch, CPU_SAMPLE_SECONDS)
+    ref_mode = None if args.no_ref_mode else run_ref_mode(args, ctx, stream)
     serve = None
     if not args.no_serve:
         himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
@@ -434,7 +440,8 @@ def run_ours(args, dist):
                 "tile_stats": {"tiles": stats["tiles"], "visits_per_tile": stats["tile_visits"] / max(1, stats["tiles"]),
                                "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},
                 "gpu_launches": 3 * args.steps,
-                "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serve": serve}
+                "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serve": serve,
+                "ref_mode": ref_mode}
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()

@@ -65,6 +65,11 @@ class Context:
     def sync(self, stream=None):
         self.check(lib().dtb_sync(self._h, ctypes.c_void_p(_stream_ptr(stream))))
 
+    def inject_queue_stall(self, timeout_ms):
+        """Failure-detection self-test: the next tile run of this context waits on a tile that is never queued,
+        so its bounded queue wait (``timeout_ms``) ends the run with DTB_ERR_TIMEOUT (dtb_debug_inject_queue_stall)."""
+        self.check(lib().dtb_debug_inject_queue_stall(self._h, int(timeout_ms)))
+
     def close(self):
         if self._h:
             lib().dtb_context_destroy(self._h)

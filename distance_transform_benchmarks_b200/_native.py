@@ -29,7 +29,7 @@ DTB_SYMBOLS = [
     "dtb_device_to_host", "dtb_context_set_tuning", "dtb_context_get_tuning", "dtb_plan_create", "dtb_plan_run",
     "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy", "dtb_serve_create", "dtb_serve_submit", "dtb_serve_poll",
     "dtb_serve_release", "dtb_serve_get_stats", "dtb_serve_destroy", "dtb_gdt_ref_blocks", "dtb_image_alloc",
-    "dtb_image_free",
+    "dtb_image_free", "dtb_debug_inject_queue_stall",
 ]
 
 DTB_REQ_IMAGE = 0
@@ -127,6 +127,8 @@ def lib():
         L.dtb_gdt_ref_blocks.argtypes = [P, IMG, IMG, IMG, F, F, P, U32, P]
         L.dtb_image_alloc.restype = I32
         L.dtb_image_alloc.argtypes = [I32, I32, I32, I32, ctypes.POINTER(DtbImage)]
+        L.dtb_debug_inject_queue_stall.restype = I32
+        L.dtb_debug_inject_queue_stall.argtypes = [P, U32]
         L.dtb_image_free.restype = I32
         L.dtb_image_free.argtypes = [ctypes.POINTER(DtbImage)]
         L.dtb_gdt_batch.restype = I32

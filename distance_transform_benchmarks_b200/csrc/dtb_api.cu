@@ -128,6 +128,10 @@ __global__ void __launch_bounds__(256) ggdt_add_counts(int32_t* __restrict__ cou
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) counts[t] += add[t];
 }
 
+// dtb_debug_inject_queue_stall: counts one queued tile that is never pushed, so `pending` cannot reach 0 and the
+// workers idle in queue_pop until the no-progress watchdog sets DERR_QUEUE_TIMEOUT and every worker returns.
+__global__ void ggdt_phantom_pending(QueueHdr* hdr) { atomicAdd(&hdr->pending.v, 1u); }
+
 // Tiles never reached keep uninitialised memory: write v there.
 __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
                                                      int n, uint32_t total, const uint32_t* __restrict__ states) {
@@ -312,17 +316,19 @@ uint64_t tuning_key(int n, uint32_t total) {
   return ((uint64_t)next_pow2((uint32_t)std::max(n, 1)) << 32) | next_pow2(std::max<uint32_t>(total, 1));
 }
 
-Queue make_queue(uint8_t* dbase, const ScratchLayout& L) {
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns) {
   const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * L.total + (1ull << 20));
   // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
   // this cap, which only turns a scheduling bug into an error instead of an endless run.
   return Queue{reinterpret_cast<QueueHdr*>(dbase + L.o_hdr), reinterpret_cast<uint32_t*>(dbase + L.o_ring), L.cap - 1,
-               DEFAULT_TIMEOUT_NS, (uint32_t)cap_visits, L.total};
+               timeout_ns, (uint32_t)cap_visits, L.total};
 }
 
 dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
                               cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1) {
-  Queue q = make_queue(dbase, L);
+  const uint64_t stall_ns = ctx->inject_stall_ns;
+  ctx->inject_stall_ns = 0;
+  Queue q = make_queue(dbase, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS);
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + L.o_desc);
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
   const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
@@ -335,6 +341,10 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
   const uint32_t scan_blocks = std::min<uint32_t>((total + 3) / 4, (uint32_t)ctx->num_sms * 16);
   ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q, nullptr, 0);
   DTB_CUDA(ctx, cudaGetLastError());
+  if (stall_ns) {
+    ggdt_phantom_pending<<<1, 1, 0, stream>>>(q.hdr);
+    DTB_CUDA(ctx, cudaGetLastError());
+  }
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(resident_workers(ctx, mode, t) / PERSIST_WPC);
   cfg.blockDim = dim3(PERSIST_WPC * 32);
@@ -850,6 +860,13 @@ static dtb_status copy2d(const dtb_image* src, const dtb_image* dst, cudaMemcpyK
                                     (size_t)src->width * src->elem_size, (size_t)src->height, kind, st);
   if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(st);
   return e == cudaSuccess ? DTB_OK : DTB_ERR_CUDA;
+}
+
+DTB_API dtb_status dtb_debug_inject_queue_stall(dtb_context ctx, uint32_t timeout_ms) {
+  if (!ctx || timeout_ms == 0 || timeout_ms > 60000) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->inject_stall_ns = (uint64_t)timeout_ms * 1000000ull;
+  return DTB_OK;
 }
 
 DTB_API dtb_status dtb_image_alloc(int32_t width, int32_t height, int32_t elem_size, int32_t memory_kind, dtb_image* out) {

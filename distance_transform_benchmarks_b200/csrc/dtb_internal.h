@@ -111,6 +111,8 @@ struct dtb_context_s {
   int32_t* dround_counts = nullptr;
   size_t dround_counts_size = 0;
   bool count_rounds = false;
+  // dtb_debug_inject_queue_stall: no-progress limit of the next persistent run (0 = no injection, one-shot).
+  uint64_t inject_stall_ns = 0;
   std::mutex mu;
 };
 
@@ -160,7 +162,7 @@ struct RepitchItem {
   uint32_t row_base;  // prefix of rows over the items of the launch
 };
 __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restrict__ items, int n, uint32_t total_rows);
-Queue make_queue(uint8_t* dbase, const ScratchLayout& L);
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns = DEFAULT_TIMEOUT_NS);
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
 uint64_t tuning_key(int n, uint32_t total);
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);

@@ -199,6 +199,12 @@ DTB_API void dtb_serve_destroy(dtb_server s);
 DTB_API dtb_status dtb_gdt_noalloc(const dtb_image* img, const dtb_image* mask, const dtb_image* dist, float gamma,
                                    float v, void* stream);
 
+/* Failure-detection self-test (host-side injection, no device fault): the next persistent tile run of this
+ * context counts one queued tile that is never pushed and uses timeout_ms (1..60000) as the no-progress limit
+ * of its tile queue.  Its workers find no work, the bounded wait in every worker ends, the kernel returns and
+ * the call reports DTB_ERR_TIMEOUT; the context stays usable for the next call.  One-shot. */
+DTB_API dtb_status dtb_debug_inject_queue_stall(dtb_context ctx, uint32_t timeout_ms);
+
 /* Pitched image storage, reference dt::image2d<T> allocation (dt/include/dt/image2d.hpp:36-50,
  * details/image2d_data_gpu.hpp:23-39).  DTB_GPU: device memory of the current device, pitch rounded up to
  * 128 bytes (the alignment the tile kernel's bulk tensor copies read fastest); DTB_CPU: host memory, pitch =

@@ -50,6 +50,21 @@ def test_invalid_arguments_are_rejected_before_any_device_work():
     a = _native.DtbImage(None, 4, 4, 4, 1, 0)
     b = _native.DtbImage(None, 4, 4, 4, 1, 0)  # both CPU: not a host->device pair
     assert lib.dtb_host_to_device(ctypes.byref(a), ctypes.byref(b), None) == 1
+    assert lib.dtb_gdt_ref_blocks(None, None, None, None, 0.5, 1.0, None, 0, None) == 1
+    assert lib.dtb_debug_inject_queue_stall(None, 100) == 1
+
+
+def test_host_image_allocation_without_gpu():
+    """dtb_image_alloc / dtb_image_free of CPU images: packed rows like the reference's CPU image2d."""
+    lib = _native.lib()
+    im = _native.DtbImage()
+    assert lib.dtb_image_alloc(7, 5, 3, 0, ctypes.byref(im)) == 0
+    assert (im.width, im.height, im.pitch, im.elem_size, im.memory_kind) == (7, 5, 21, 3, 0) and im.buffer
+    ctypes.memset(im.buffer, 0xAB, im.pitch * im.height)
+    assert lib.dtb_image_free(ctypes.byref(im)) == 0 and not im.buffer
+    assert lib.dtb_image_alloc(-1, 5, 1, 0, ctypes.byref(im)) == 1
+    assert lib.dtb_image_alloc(4, 4, 1, 7, ctypes.byref(im)) == 1
+    assert lib.dtb_image_free(None) == 1
 
 
 def test_host_library_exports():
