@@ -380,9 +380,8 @@ def run_ours(args, dist):
     e2e = None
     himgs = hmasks = hdists = None
     if not args.no_e2e:
-        himgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
-        hmasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]
-        hdists = [torch.empty(i.shape[:2], dtype=torch.float32).pin_memory() for i, _, _ in batch]
+        # The batch as a data loader would hand it over: one pinned arena per plane kind (images, masks, maps).
+        himgs, hmasks, hdists = dtb.host_batch_arena([i for i, _, _ in batch], [m for _, m, _ in batch])
         h2d = sum(t.numel() * t.element_size() for t in himgs + hmasks)
         d2h = sum(t.numel() * t.element_size() for t in hdists)
 
@@ -403,6 +402,20 @@ def run_ours(args, dist):
                "ms_per_step": ems}
         ok = all(torch.equal(hd, d.cpu()) for hd, d in zip(hdists[:8], dists[:8]))
         e2e["matches_device_run"] = bool(ok)
+        e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
+        # The same batch from separate pinned buffers per image (one copy per plane and direction).
+        simgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
+        smasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]
+        sdists = [torch.empty(i.shape[:2], dtype=torch.float32).pin_memory() for i, _, _ in batch]
+        dtb.geodesic_distance_transform_batch(simgs, smasks, gammas, dists=sdists, ctx=ctx, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            dtb.geodesic_distance_transform_batch(simgs, smasks, gammas, dists=sdists, ctx=ctx, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e["separate_buffers_mpx_s"] = px / 1e6 / (e0.elapsed_time(e1) / 3 / 1e3)
+        simgs = smasks = sdists = None
 
     kms = statistics.mean(kernel_ms) if kernel_ms and kernel_ms[0] > 0 else None
     peak, peak_kind = measured_peak_gbs()

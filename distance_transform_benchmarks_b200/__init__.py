@@ -127,6 +127,41 @@ def image_view(t, elem_size=None):
     return DtbImage(t.data_ptr() if t.numel() else None, w, h, pitch, es, kind)
 
 
+# dtb_image as a numpy record (same layout: 8-byte pointer, five int32, padded to 32 bytes).
+_VIEW_DTYPE = np.dtype([("buffer", "<u8"), ("width", "<i4"), ("height", "<i4"), ("pitch", "<i4"), ("elem_size", "<i4"),
+                        ("memory_kind", "<i4")], align=True)
+assert _VIEW_DTYPE.itemsize == ctypes.sizeof(DtbImage)
+
+
+def _batch_views(tensors, elem_sizes):
+    """dtb_image array for a list of tensors (the same checks as image_view, one pass, no ctypes objects per
+    image: a 1024-image batch costs about a third of building image_view structs one by one).  `elem_sizes`:
+    the bytes per pixel allowed (e.g. (1, 3) for gray or rgb8 images)."""
+    rows = []
+    for t in tensors:
+        shp = t.shape
+        st = t.stride()
+        nd = len(shp)
+        if nd == 3:
+            h, w, c = shp
+            if st[2] != 1 or st[1] != c:
+                raise ValueError("pixels of a [H, W, C] image must be contiguous")
+        elif nd == 2:
+            h, w = shp
+            c = 1
+            if st[1] != 1 and w > 1:
+                raise ValueError("rows must be contiguous")
+        else:
+            raise ValueError("expected a [H, W] or [H, W, C] tensor")
+        es = t.element_size()
+        if es * c not in elem_sizes:
+            raise ValueError("element size %d, expected one of %s" % (es * c, elem_sizes))
+        rows.append((t.data_ptr() if h * w else 0, w, h, st[0] * es if h > 1 else w * es * c, es * c,
+                     DTB_GPU if t.is_cuda else DTB_CPU))
+    arr = np.array(rows, dtype=_VIEW_DTYPE)
+    return arr, arr.ctypes.data_as(ctypes.POINTER(DtbImage))
+
+
 PITCH_ALIGN = 128  # bytes; cudaMallocPitch-style rows, as the reference's GPU image2d (image2d_data_gpu.hpp:28)
 
 
@@ -140,6 +175,35 @@ def pitched_empty(height, width, channels=1, dtype=torch.uint8, device="cuda"):
     if channels == 1:
         return store[:height, :width]
     return torch.as_strided(store, (height, width, channels), (pitch_elems, channels, 1))
+
+
+def host_batch_arena(imgs, masks, pin=True):
+    """Packs a batch's host images and masks back to back into one (pinned) buffer per plane kind and allocates the
+    distance maps back to back in a third one; returns (img_views, mask_views, dist_views), tensors viewing the
+    arenas.  Adjacent packed planes are what the host-buffer pipeline moves as one copy per chunk and direction
+    (a data loader that fills such arenas gets the full copy-engine bandwidth in both directions)."""
+    imgs = [_as_tensor(i) for i in imgs]
+    masks = [_as_tensor(m) for m in masks]
+
+    def arena(shapes, dtype):
+        sizes = [int(np.prod(shp)) for shp in shapes]
+        buf = torch.empty(max(1, sum(sizes)), dtype=dtype)
+        if pin:
+            buf = buf.pin_memory()
+        views, off = [], 0
+        for shp, n in zip(shapes, sizes):
+            views.append(buf[off:off + n].view(*shp))
+            off += n
+        return views
+
+    iv = arena([tuple(t.shape) for t in imgs], torch.uint8)
+    mv = arena([tuple(t.shape) for t in masks], torch.uint8)
+    dv = arena([tuple(t.shape[:2]) for t in imgs], torch.float32)
+    for a, b in zip(iv, imgs):
+        a.copy_(b)
+    for a, b in zip(mv, masks):
+        a.copy_(b)
+    return iv, mv, dv
 
 
 def pitched_from(arr, device="cuda"):
@@ -239,13 +303,16 @@ def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=No
     ctx = _ctx_for(imgs[0], ctx)
     if stream is None and imgs[0].is_cuda:
         stream = torch.cuda.current_stream(imgs[0].device)
-    vi = (DtbImage * n)(*[image_view(t, 3 if t.dim() == 3 else 1) for t in imgs])
-    vm = (DtbImage * n)(*[image_view(t, 1) for t in masks])
-    vd = (DtbImage * n)(*[image_view(t, 4) for t in dists])
-    g = (ctypes.c_float * n)(*[float(x) for x in gammas])
+    if len(masks) != n or len(dists) != n or len(gammas) != n:
+        raise ValueError("imgs, masks, gammas and dists must have the same length")
+    keep_i, vi = _batch_views(imgs, (1, 3))
+    keep_m, vm = _batch_views(masks, (1,))
+    keep_d, vd = _batch_views(dists, (4,))
+    g = np.asarray(gammas, dtype=np.float32)
     flags = (DTB_FLAG_ROUNDS if rounds else 0) | (DTB_FLAG_ASYNC if asynchronous else 0) | \
         (DTB_FLAG_TIMING if timing else 0)
-    ctx.check(lib().dtb_gdt_batch(ctx.handle, n, vi, vm, vd, g, float(v), flags, ctypes.c_void_p(_stream_ptr(stream))))
+    ctx.check(lib().dtb_gdt_batch(ctx.handle, n, vi, vm, vd, g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(v),
+                                  flags, ctypes.c_void_p(_stream_ptr(stream))))
     return dists
 
 

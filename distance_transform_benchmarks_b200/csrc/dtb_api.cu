@@ -660,6 +660,7 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
     if (e) cudaEventDestroy(e);
   if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
   if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
+  if (ctx->s_lane) cudaStreamDestroy(ctx->s_lane);
   delete ctx;
 }
 

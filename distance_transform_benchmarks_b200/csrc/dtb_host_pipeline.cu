@@ -1,11 +1,15 @@
 // dtb_host_pipeline.cu -- batches whose images, masks and distance maps are all in host memory.
 //
-// Host-to-device copies with a pitch change crawl (the copy engines move one narrow row at a time), so the
-// pipeline copies every image and mask as one 1-D block into packed device memory, moves rows into 128-byte
-// pitches on the device only where the TMA needs it (rows not a multiple of 16 bytes), and writes distances
-// packed so that each map returns as one 1-D block.  The batch is cut into chunks of about host_chunk_px
-// pixels; the copies in (stream s_in), the tile runs (the caller's stream) and the copies out (stream s_out)
-// of successive chunks overlap.
+// Host-to-device copies with a pitch change crawl (the copy engines move one narrow row at a time), and many
+// small copies in both directions overlap poorly, so the pipeline moves each run of planes that are packed and
+// adjacent in host memory (a batch in one pinned arena is one run per plane kind) as ONE 1-D copy into device
+// staging that mirrors the host bytes, moves rows into 128-byte pitches on the device only where the TMA needs
+// it (rows or bases not on 16 bytes), and writes distances packed in the mirrored layout so that each run
+// returns as one 1-D copy.  The batch is cut into chunks of about host_chunk_px pixels; the copies in (stream
+// s_in), the tile runs and the copies out (stream s_out) of successive chunks overlap.  The tile runs alternate
+// between two compute lanes (the caller's stream and s_lane), each launched on half of the co-resident CTAs:
+// a run's tail, where only the last tiles of its largest images are still active, then overlaps the next
+// chunk's run instead of idling the GPU (one lane ran each chunk at about a third of the batch rate).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,14 +58,70 @@ cudaEvent_t event_at(dtb_context ctx, size_t i) {
   return ctx->evpool[i];
 }
 
-struct Plane {  // device placement of one image's planes
-  uint8_t* img_packed;
-  uint8_t* img_tma;   // == img_packed when the packed rows are TMA-aligned
-  uint8_t* mask_packed;
-  uint8_t* mask_tma;
-  float* dist;        // packed rows of 4 * width bytes
-  int64_t img_pitch, mask_pitch;
+// One host <-> device copy of the pipeline: 1-D when rows == 1 (a run of adjacent packed planes), else 2-D.
+// `dev` is an offset into the staging block.
+struct Copy {
+  size_t dev;
+  uint8_t* host;
+  size_t host_pitch, dev_pitch, width, rows;
 };
+
+dtb_status issue(dtb_context ctx, const Copy& c, uint8_t* stage, bool to_device, cudaStream_t st) {
+  uint8_t* d = stage + c.dev;
+  if (to_device) {
+    if (c.rows == 1) DTB_CUDA(ctx, cudaMemcpyAsync(d, c.host, c.width, cudaMemcpyHostToDevice, st));
+    else DTB_CUDA(ctx, cudaMemcpy2DAsync(d, c.dev_pitch, c.host, c.host_pitch, c.width, c.rows, cudaMemcpyHostToDevice, st));
+  } else {
+    if (c.rows == 1) DTB_CUDA(ctx, cudaMemcpyAsync(c.host, d, c.width, cudaMemcpyDeviceToHost, st));
+    else DTB_CUDA(ctx, cudaMemcpy2DAsync(c.host, c.host_pitch, d, c.dev_pitch, c.width, c.rows, cudaMemcpyDeviceToHost, st));
+  }
+  return DTB_OK;
+}
+
+// Host side of one plane of one image.
+struct HostPlane {
+  const uint8_t* ptr;
+  size_t pitch, row_bytes, rows;
+  bool empty() const { return row_bytes == 0 || rows == 0; }
+  bool packed() const { return pitch == row_bytes; }
+  size_t bytes() const { return row_bytes * rows; }
+};
+
+// Device placement of one kind of plane (images, masks or distances) for the images [a, b) of a chunk.  Runs of
+// consecutive packed planes that are adjacent in host memory move as ONE 1-D copy: their device staging mirrors
+// the host byte range, at an offset congruent to the host address modulo 256, so each plane keeps the
+// alignment it has on the host (few large copies overlap in both directions on the copy engines; per-image
+// copies do not).  Planes with padded host rows get their own packed region and a 2-D copy.  `take(bytes)`
+// returns 256-byte aligned offsets into the staging block; dev_off[i] receives the plane's offset.
+template <class Take>
+void place_plane(int a, int b, const std::vector<HostPlane>& hp, Take&& take, std::vector<size_t>& dev_off,
+                 std::vector<Copy>& copies) {
+  int i = a;
+  while (i < b) {
+    if (hp[i].empty()) { ++i; continue; }
+    if (!hp[i].packed()) {
+      dev_off[i] = take(hp[i].bytes());
+      copies.push_back(Copy{dev_off[i], const_cast<uint8_t*>(hp[i].ptr), hp[i].pitch, hp[i].row_bytes, hp[i].row_bytes,
+                            hp[i].rows});
+      ++i;
+      continue;
+    }
+    const uint8_t* start = hp[i].ptr;
+    const uint8_t* end = start + hp[i].bytes();
+    int j = i + 1;
+    for (; j < b; ++j) {
+      if (hp[j].empty()) continue;
+      if (!hp[j].packed() || hp[j].ptr != end) break;
+      end += hp[j].bytes();
+    }
+    const size_t shift = reinterpret_cast<uintptr_t>(start) & 255u;
+    const size_t region = take((size_t)(end - start) + shift) + shift;
+    for (int m = i; m < j; ++m)
+      if (!hp[m].empty()) dev_off[m] = region + (size_t)(hp[m].ptr - start);
+    copies.push_back(Copy{region, const_cast<uint8_t*>(start), 0, 0, (size_t)(end - start), 1});
+    i = j;
+  }
+}
 
 }  // namespace
 
@@ -70,44 +130,7 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   const int n = (int)jobs.size();
   if (!ctx->s_in) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
-
-  // ---- device placement of the planes ----
-  std::vector<Plane> pl(n);
-  size_t off = 0;
-  auto take = [&](size_t bytes) {
-    const size_t o = off;
-    off = align_up(off + std::max<size_t>(bytes, 1), 256);
-    return o;
-  };
-  std::vector<size_t> o_ip(n), o_it(n), o_mp(n), o_mt(n), o_d(n);
-  for (int i = 0; i < n; ++i) {
-    const Job& j = jobs[i];
-    const size_t rb = (size_t)j.width * j.channels, h = (size_t)j.height;
-    const size_t prb = align_up(rb, 128), pmb = align_up((size_t)j.width, 128);
-    o_ip[i] = take(rb * h);
-    o_it[i] = (rb % 16) ? take(prb * h) : o_ip[i];
-    o_mp[i] = take((size_t)j.width * h);
-    o_mt[i] = (j.width % 16) ? take(pmb * h) : o_mp[i];
-    o_d[i] = take(4 * (size_t)j.width * h);
-    pl[i].img_pitch = (rb % 16) ? (int64_t)prb : (int64_t)rb;
-    pl[i].mask_pitch = (j.width % 16) ? (int64_t)pmb : (int64_t)j.width;
-  }
-  dtb_status s = grow(ctx, &ctx->dstage, &ctx->dstage_size, off);
-  if (s != DTB_OK) return s;
-  uint8_t* stage = static_cast<uint8_t*>(ctx->dstage);
-  for (int i = 0; i < n; ++i) {
-    pl[i].img_packed = stage + o_ip[i];
-    pl[i].img_tma = stage + o_it[i];
-    pl[i].mask_packed = stage + o_mp[i];
-    pl[i].mask_tma = stage + o_mt[i];
-    pl[i].dist = reinterpret_cast<float*>(stage + o_d[i]);
-    jobs[i].img = pl[i].img_tma;
-    jobs[i].img_pitch = pl[i].img_pitch;
-    jobs[i].mask = pl[i].mask_tma;
-    jobs[i].mask_pitch = pl[i].mask_pitch;
-    jobs[i].dist = pl[i].dist;
-    jobs[i].dist_pitch = 4 * (int64_t)jobs[i].width;
-  }
+  if (!ctx->s_lane) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_lane, cudaStreamNonBlocking));
 
   // ---- chunks of about host_chunk_px pixels ----
   std::vector<int> cut{0};
@@ -121,6 +144,49 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   }
   cut.push_back(n);
   const int nchunks = (int)cut.size() - 1;
+
+  // ---- device placement of the planes: mirrored runs, repitched copies where the TMA needs them ----
+  std::vector<HostPlane> hi(n), hm(n), hd(n);
+  for (int i = 0; i < n; ++i) {
+    const Job& j = jobs[i];
+    const size_t w = (size_t)j.width, h = (size_t)j.height;
+    hi[i] = HostPlane{static_cast<const uint8_t*>(imgs[i]->buffer), (size_t)imgs[i]->pitch, w * j.channels, h};
+    hm[i] = HostPlane{static_cast<const uint8_t*>(masks[i]->buffer), (size_t)masks[i]->pitch, w, h};
+    hd[i] = HostPlane{static_cast<const uint8_t*>(dists[i]->buffer), (size_t)dists[i]->pitch, 4 * w, h};
+  }
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + std::max<size_t>(bytes, 1), 256);
+    return o;
+  };
+  std::vector<size_t> o_ip(n, 0), o_it(n, 0), o_mp(n, 0), o_mt(n, 0), o_d(n, 0);
+  std::vector<std::vector<Copy>> cin(nchunks), cout(nchunks);
+  for (int k = 0; k < nchunks; ++k) {
+    place_plane(cut[k], cut[k + 1], hi, take, o_ip, cin[k]);
+    place_plane(cut[k], cut[k + 1], hm, take, o_mp, cin[k]);
+    place_plane(cut[k], cut[k + 1], hd, take, o_d, cout[k]);
+  }
+  for (int i = 0; i < n; ++i) {
+    const Job& j = jobs[i];
+    if (j.width == 0 || j.height == 0) continue;
+    const size_t rb = (size_t)j.width * j.channels, h = (size_t)j.height;
+    // The tile kernel reads images and masks through TMA maps: 16-byte aligned base and pitch.
+    o_it[i] = (rb % 16 || o_ip[i] % 16) ? take(align_up(rb, 128) * h) : o_ip[i];
+    o_mt[i] = ((size_t)j.width % 16 || o_mp[i] % 16) ? take(align_up((size_t)j.width, 128) * h) : o_mp[i];
+  }
+  dtb_status s = grow(ctx, &ctx->dstage, &ctx->dstage_size, off);
+  if (s != DTB_OK) return s;
+  uint8_t* stage = static_cast<uint8_t*>(ctx->dstage);
+  for (int i = 0; i < n; ++i) {
+    const int64_t rb = (int64_t)jobs[i].width * jobs[i].channels;
+    jobs[i].img = stage + o_it[i];
+    jobs[i].img_pitch = (o_it[i] == o_ip[i]) ? rb : (int64_t)align_up((size_t)rb, 128);
+    jobs[i].mask = stage + o_mt[i];
+    jobs[i].mask_pitch = (o_mt[i] == o_mp[i]) ? (int64_t)jobs[i].width : (int64_t)align_up((size_t)jobs[i].width, 128);
+    jobs[i].dist = reinterpret_cast<float*>(stage + o_d[i]);
+    jobs[i].dist_pitch = 4 * (int64_t)jobs[i].width;
+  }
 
   // ---- per-chunk scratch, tables and repitch lists, all uploaded in one copy ----
   LaunchTuning tuning = ctx->tuning;
@@ -145,13 +211,13 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
       const Job& j = jobs[i];
       if (j.width == 0 || j.height == 0) continue;
       const uint32_t rb = (uint32_t)(j.width * j.channels);
-      if (pl[i].img_tma != pl[i].img_packed) {
-        items[k].push_back({pl[i].img_packed, pl[i].img_tma, rb, (uint32_t)j.height, (uint32_t)pl[i].img_pitch, rows[k]});
+      if (o_it[i] != o_ip[i]) {
+        items[k].push_back({stage + o_ip[i], stage + o_it[i], rb, (uint32_t)j.height, (uint32_t)j.img_pitch, rows[k]});
         rows[k] += (uint32_t)j.height;
       }
-      if (pl[i].mask_tma != pl[i].mask_packed) {
-        items[k].push_back({pl[i].mask_packed, pl[i].mask_tma, (uint32_t)j.width, (uint32_t)j.height,
-                            (uint32_t)pl[i].mask_pitch, rows[k]});
+      if (o_mt[i] != o_mp[i]) {
+        items[k].push_back({stage + o_mp[i], stage + o_mt[i], (uint32_t)j.width, (uint32_t)j.height, (uint32_t)j.mask_pitch,
+                            rows[k]});
         rows[k] += (uint32_t)j.height;
       }
     }
@@ -179,53 +245,33 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   // ---- the pipeline ----
   DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ev_tables, 0));  // staging memory is free once earlier work is done
   for (int k = 0; k < nchunks; ++k) {
-    for (int i = cut[k]; i < cut[k + 1]; ++i) {
-      const dtb_image* ui = imgs[i];
-      const dtb_image* um = masks[i];
-      const Job& j = jobs[i];
-      if (j.width == 0 || j.height == 0) continue;
-      const size_t rb = (size_t)j.width * j.channels;
-      if ((size_t)ui->pitch == rb)
-        DTB_CUDA(ctx, cudaMemcpyAsync(pl[i].img_packed, ui->buffer, rb * j.height, cudaMemcpyHostToDevice, ctx->s_in));
-      else
-        DTB_CUDA(ctx, cudaMemcpy2DAsync(pl[i].img_packed, rb, ui->buffer, ui->pitch, rb, j.height, cudaMemcpyHostToDevice,
-                                        ctx->s_in));
-      if (um->pitch == j.width)
-        DTB_CUDA(ctx, cudaMemcpyAsync(pl[i].mask_packed, um->buffer, (size_t)j.width * j.height, cudaMemcpyHostToDevice,
-                                      ctx->s_in));
-      else
-        DTB_CUDA(ctx, cudaMemcpy2DAsync(pl[i].mask_packed, j.width, um->buffer, um->pitch, j.width, j.height,
-                                        cudaMemcpyHostToDevice, ctx->s_in));
-    }
+    for (const Copy& c : cin[k])
+      if ((s = issue(ctx, c, stage, true, ctx->s_in)) != DTB_OK) return s;
     cudaEvent_t e_in = event_at(ctx, 1 + 3 * k);
     if (!e_in) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
     DTB_CUDA(ctx, cudaEventRecord(e_in, ctx->s_in));
   }
+  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_lane, ev_tables, 0));
+  const int lanes = nchunks > 1 ? 2 : 1;
+  LaunchTuning lane_tuning = tuning;
+  lane_tuning.grid_percent = std::max(1, tuning.grid_percent / lanes);
   for (int k = 0; k < nchunks; ++k) {
     uint8_t* cbase = scratch + o_chunk[k];
-    DTB_CUDA(ctx, cudaStreamWaitEvent(stream, event_at(ctx, 1 + 3 * k), 0));
+    cudaStream_t lane = (k % lanes) ? ctx->s_lane : stream;
+    DTB_CUDA(ctx, cudaStreamWaitEvent(lane, event_at(ctx, 1 + 3 * k), 0));
     if (!items[k].empty()) {
       const uint32_t blocks = std::min<uint32_t>((rows[k] + 7) / 8, (uint32_t)ctx->num_sms * 8);
-      repitch_rows<<<blocks, 256, 0, stream>>>(reinterpret_cast<const RepitchItem*>(scratch + o_items[k]),
-                                              (int)items[k].size(), rows[k]);
+      repitch_rows<<<blocks, 256, 0, lane>>>(reinterpret_cast<const RepitchItem*>(scratch + o_items[k]),
+                                            (int)items[k].size(), rows[k]);
       DTB_CUDA(ctx, cudaGetLastError());
     }
-    if ((s = enqueue_persistent(ctx, cbase, L[k], MODE_NS, tuning, stream, nullptr, nullptr)) != DTB_OK) return s;
+    if ((s = enqueue_persistent(ctx, cbase, L[k], MODE_NS, lane_tuning, lane, nullptr, nullptr)) != DTB_OK) return s;
     cudaEvent_t e_run = event_at(ctx, 2 + 3 * k);
     if (!e_run) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
-    DTB_CUDA(ctx, cudaEventRecord(e_run, stream));
+    DTB_CUDA(ctx, cudaEventRecord(e_run, lane));
     DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_out, e_run, 0));
-    for (int i = cut[k]; i < cut[k + 1]; ++i) {
-      const dtb_image* ud = dists[i];
-      const Job& j = jobs[i];
-      if (j.width == 0 || j.height == 0) continue;
-      const size_t rb = 4 * (size_t)j.width;
-      if ((size_t)ud->pitch == rb)
-        DTB_CUDA(ctx, cudaMemcpyAsync(ud->buffer, pl[i].dist, rb * j.height, cudaMemcpyDeviceToHost, ctx->s_out));
-      else
-        DTB_CUDA(ctx, cudaMemcpy2DAsync(ud->buffer, ud->pitch, pl[i].dist, rb, rb, j.height, cudaMemcpyDeviceToHost,
-                                        ctx->s_out));
-    }
+    for (const Copy& c : cout[k])
+      if ((s = issue(ctx, c, stage, false, ctx->s_out)) != DTB_OK) return s;
   }
   cudaEvent_t e_done = event_at(ctx, 3 + 3 * (nchunks - 1));
   if (!e_done) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");

@@ -103,10 +103,10 @@ struct dtb_context_s {
   bool async_pending = false;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
   bool timed = false;
-  // Host-buffer pipeline: copy streams, events, chunk size in pixels.
-  cudaStream_t s_in = nullptr, s_out = nullptr;
+  // Host-buffer pipeline: copy streams, a second compute lane, events, chunk size in pixels.
+  cudaStream_t s_in = nullptr, s_out = nullptr, s_lane = nullptr;
   std::vector<cudaEvent_t> evpool;
-  uint64_t host_chunk_px = 32ull << 20;
+  uint64_t host_chunk_px = 16ull << 20;
   // dtb_gdt_ref_blocks: per-tile round counters of the running call (device scratch of `total` int32).
   int32_t* dround_counts = nullptr;
   size_t dround_counts_size = 0;

@@ -87,8 +87,8 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
  * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128; 0 = keep);
  * grid_percent: share of the co-resident CTAs launched, 1..100 (fewer workers re-visit fewer tiles on
  * narrow fronts; 0 = 100); host_chunk_kpx: pixels (in units of 1024) per chunk of the pipeline that serves
- * batches in host memory (host-to-device copies, tile runs and device-to-host copies of successive chunks
- * overlap; 0 = keep, default 32768). */
+ * batches in host memory (host-to-device copies, tile runs on two alternating compute lanes and
+ * device-to-host copies of successive chunks overlap; 0 = keep, default 16384). */
 typedef struct dtb_tuning {
   int32_t ctas_per_sm;
   int32_t grid_percent;

@@ -220,6 +220,29 @@ def test_host_pipeline_many_chunks_padded_rows_and_empty_images():
     c.close()
 
 
+@pytest.mark.parametrize("chunk_kpx", [16, 32768])
+def test_host_pipeline_arena_runs(chunk_kpx):
+    """Batch in one host arena per plane kind: adjacent packed planes move as one copy per chunk; odd widths put
+    most planes off 16-byte boundaries (repitched on the device); small chunks split the runs; one image outside
+    the arena breaks a run."""
+    c = dtb.Context(0)
+    c.set_tuning(host_chunk_kpx=chunk_kpx)
+    rng = np.random.default_rng(21)
+    batch = []
+    for k in range(23):
+        w, h = int(rng.integers(1, 180)), int(rng.integers(1, 150))
+        img = wl.voronoi_rgb(k, w, h) if k % 3 == 0 else wl.blobs_gray(k, w, h)
+        batch.append((img, wl.random_disks(rng, w, h, 2, 1, 4), float(rng.choice([0.01, 0.1, 1.0]))))
+    iv, mv, dv = dtb.host_batch_arena([i for i, _, _ in batch], [m for _, m, _ in batch])
+    iv[11] = torch.from_numpy(batch[11][0].copy())  # outside the arena: its own copy
+    dtb.geodesic_distance_transform_batch(iv, mv, [g for _, _, g in batch], dists=dv, ctx=c)
+    for k, (img, mask, g) in enumerate(batch):
+        assert_images_eq(dv[k], orc.ggdt_ns(img, mask, g), "arena image %d" % k)
+    if chunk_kpx == 16:
+        assert c.stats()["rounds"] > 3
+    c.close()
+
+
 def test_batch_host_buffers(ctx):
     batch = wl.config3(seed=12, n=6, smin=40, smax=200)
     dists = dtb.geodesic_distance_transform_batch([torch.from_numpy(i) for i, _, _ in batch],
@@ -290,7 +313,7 @@ def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
 def test_every_tuning_gives_the_same_map(ctas, pct):
     c = dtb.Context(0)
     c.set_tuning(ctas_per_sm=ctas, grid_percent=pct)
-    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 32768}
+    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 16384}
     img, mask, gamma = wl.config0(seed=9)
     d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=c)
     assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), "tuning %d/%d" % (ctas, pct))
