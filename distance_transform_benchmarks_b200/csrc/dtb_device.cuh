@@ -19,6 +19,10 @@ constexpr int TILE = 32;                  // tile side (pixels); one warp owns o
 constexpr int IMG_BOX_ROWS = TILE + 2;    // image box rows: 1-pixel halo above and below
 constexpr int IMG_BOX_GRAY = 64;          // gray box width (bytes): x0-16 .. x0+47 covers x0-1 .. x0+32
 constexpr int IMG_BOX_RGB = 128;          // rgb8 box width (bytes): 3*x0-16 .. 3*x0+111 covers 3*(x0-1) .. 3*(x0+33)
+// Gray visits keep a 256-entry weight table (1 KB) in the image box past the 34 x 64-byte gray rows.
+constexpr int GRAY_LUT_OFFSET = 2304;
+static_assert(GRAY_LUT_OFFSET >= IMG_BOX_ROWS * IMG_BOX_GRAY && GRAY_LUT_OFFSET + 1024 <= IMG_BOX_ROWS * IMG_BOX_RGB,
+              "gray weight table must fit the unused part of the image box");
 constexpr int S_STRIDE = TILE + 1;        // padded transpose buffer stride (floats): conflict-free both ways
 
 // Tile state word: flags in the low byte, image index of the tile in the upper 24 bits.
@@ -230,10 +234,12 @@ __device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
 // ns-mode: w = sqrt(1 + g2 * dI2), dI2 = sum_c (I_c(p) - I_c(q))^2.  Pixels are packed little-endian in a
 // u32 (gray: byte 0; rgb8: bytes 0..2), unused bytes zero.  dI2 <= 3 * 255^2 is exact in fp32; each of the
 // three float operations is rounded separately (no contraction), the square root correctly rounded.
+__device__ __forceinline__ float ns_weight_sq(uint32_t dI2, float g2) {
+  return __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(g2, __uint2float_rn(dI2))));
+}
 __device__ __forceinline__ float ns_weight(uint32_t pa, uint32_t pb, float g2) {
   const uint32_t ad = __vabsdiffu4(pa, pb);
-  const uint32_t dI2 = __dp4a(ad, ad, 0u);
-  return __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(g2, __uint2float_rn(dI2))));
+  return ns_weight_sq(__dp4a(ad, ad, 0u), g2);
 }
 
 // ref-mode relaxation of one edge, reference dt/src/dt_block_passes.cuh:252-253:

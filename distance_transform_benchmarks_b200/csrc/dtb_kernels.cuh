@@ -249,30 +249,84 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   {
     const float g2 = dd.g2;
     const uint8_t* box = sm.img;
-    uint32_t pprev = box_pix(box, rgb, 0, lane);
-#pragma unroll 1
-    for (int y = 0; y <= TILE; ++y) {  // edge (y-1, y); y == 32 is the bottom halo edge
-      const uint32_t pcur = box_pix(box, rgb, y + 1, lane);
-      float w = ns_weight(pprev, pcur, g2);
-      if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
-      sm.Wv[y * W_STRIDE + lane] = w;
-      if (y < TILE) {
-        float wx = ns_weight(box_pix(box, rgb, y + 1, lane - 1), pcur, g2);
-        if (lane >= vw || y >= vh) wx = INF;
-        sm.Wh[y * W_STRIDE + lane] = wx;
+    if (!rgb) {
+      // Gray: the weight depends on |dI| in [0, 255] only.  A 256-entry table of the same expression (so the
+      // same bits) costs 8 square roots per lane instead of 65; it sits in the part of the image box that the
+      // 64-byte gray rows leave unused.
+      float* lut = reinterpret_cast<float*>(sm.img + GRAY_LUT_OFFSET);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t a = (uint32_t)(lane + 32 * k);
+        lut[a] = ns_weight_sq(a * a, g2);
       }
-      pprev = pcur;
+      __syncwarp();
+      const uint8_t* col = box + 16 + lane;  // column `lane` of the box, row r at col[r * IMG_BOX_GRAY]
+      int pprev = col[0];
+#pragma unroll 4
+      for (int y = 0; y <= TILE; ++y) {  // edge (y-1, y); y == 32 is the bottom halo edge
+        const int pcur = col[(y + 1) * IMG_BOX_GRAY];
+        float w = lut[abs(pcur - pprev)];
+        if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
+        sm.Wv[y * W_STRIDE + lane] = w;
+        if (y < TILE) {
+          float wx = lut[abs(pcur - (int)col[(y + 1) * IMG_BOX_GRAY - 1])];
+          if (lane >= vw || y >= vh) wx = INF;
+          sm.Wh[y * W_STRIDE + lane] = wx;
+        }
+        pprev = pcur;
+      }
+      const uint8_t* row = box + (lane + 1) * IMG_BOX_GRAY + 16;
+      float er = lut[abs((int)row[TILE - 1] - (int)row[TILE])];
+      if (lane >= vh || TILE - 1 >= vw) er = INF;
+      sm.Wh[lane * W_STRIDE + TILE] = er;
+    } else {
+      uint32_t pprev = box_pix(box, rgb, 0, lane);
+#pragma unroll 1
+      for (int y = 0; y <= TILE; ++y) {  // edge (y-1, y); y == 32 is the bottom halo edge
+        const uint32_t pcur = box_pix(box, rgb, y + 1, lane);
+        float w = ns_weight(pprev, pcur, g2);
+        if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
+        sm.Wv[y * W_STRIDE + lane] = w;
+        if (y < TILE) {
+          float wx = ns_weight(box_pix(box, rgb, y + 1, lane - 1), pcur, g2);
+          if (lane >= vw || y >= vh) wx = INF;
+          sm.Wh[y * W_STRIDE + lane] = wx;
+        }
+        pprev = pcur;
+      }
+      // Edge (x = 31, x = 32) of row `lane`.
+      float er = ns_weight(box_pix(box, rgb, lane + 1, TILE - 1), box_pix(box, rgb, lane + 1, TILE), g2);
+      if (lane >= vh || TILE - 1 >= vw) er = INF;
+      sm.Wh[lane * W_STRIDE + TILE] = er;
     }
-    // Edge (x = 31, x = 32) of row `lane`.
-    float er = ns_weight(box_pix(box, rgb, lane + 1, TILE - 1), box_pix(box, rgb, lane + 1, TILE), g2);
-    if (lane >= vh || TILE - 1 >= vw) er = INF;
-    sm.Wh[lane * W_STRIDE + TILE] = er;
   }
   __syncwarp();
 
   // Local fixpoint.  B overlays the image box, which is no longer needed.
   float* B = reinterpret_cast<float*>(sm.img);
-  bool any = false, ran_col = false, ran_row = false, col = true;
+  // Start in the layout whose chains begin at the halo sides that can lower the tile now: a column phase
+  // never reads the left / right halo, so a tile reached only from the side would spend its first column
+  // phase without any effect.
+  bool col = true;
+  {
+    float* pb = B + lane;
+#pragma unroll
+    for (int k = 0; k < TILE; ++k) pb[k * W_STRIDE] = d[k];
+    __syncwarp();
+    const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];
+    const bool hside = __any_sync(~0u, __fadd_rn(lft, sm.Wh[lane * W_STRIDE]) < dl ||
+                                           __fadd_rn(rgt, sm.Wh[lane * W_STRIDE + TILE]) < dr);
+    const bool vside = __any_sync(~0u, __fadd_rn(top, sm.Wv[lane]) < d[0] ||
+                                           __fadd_rn(bot, sm.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
+    if (hside && !vside) {
+      col = false;
+      const float* qb = B + lane * W_STRIDE;
+#pragma unroll
+      for (int k = 0; k < TILE; ++k) d[k] = qb[k];
+    }
+    __syncwarp();
+  }
+  bool any = false, ran_col = false, ran_row = false;
   uint32_t nph = 0;
   for (;;) {
     float wc[TILE + 1], wx[TILE];
