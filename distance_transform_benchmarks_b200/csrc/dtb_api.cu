@@ -81,13 +81,13 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
   const int lane = threadIdx.x & 31;
   WarpStats ws;
   for (;;) {
-    uint32_t t = POP_NONE, old = 0;
-    if (lane == 0) {
-      t = queue_pop(q);
-      if (t != POP_NONE) old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
-    }
-    t = __shfl_sync(~0u, t, 0);
+    const uint32_t t = queue_pop(q);
     if (t == POP_NONE) break;
+    uint32_t old = 0;
+    if (lane == 0) {
+      old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
+      if (q.keys) q.keys[t] = KEY_NONE;  // activations from here on belong to the next queue entry
+    }
     old = __shfl_sync(~0u, old, 0);
     const uint32_t img = old >> ST_IMG_SHIFT;
     const ImgDesc dd = descs[img];
@@ -250,15 +250,18 @@ uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t) {
   return ctas * PERSIST_WPC;
 }
 
-ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds) {
+ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, uint32_t buckets) {
   ScratchLayout L;
   L.n = n;
   L.total = total;
   L.cap = next_pow2(2u * (total + workers + 64u));
+  L.nb = buckets > 1 ? NBUCKET : 1u;
   size_t off = 0;
   L.o_hdr = off;    off = align_up(off + sizeof(QueueHdr), 256);
   L.o_states = off; off = align_up(off + 4ull * std::max<uint32_t>(total, 1), 256);
-  L.o_ring = off;   off = align_up(off + 4ull * L.cap, 256);
+  L.o_ring = off;   off = align_up(off + L.ring_bytes(), 256);
+  L.o_keys = off;   off = align_up(off + (L.nb > 1 ? 4ull * std::max<uint32_t>(total, 1) : 0), 256);
+  L.o_wacc = off;   off = align_up(off + (L.nb > 1 ? 8ull * (size_t)std::max(n, 1) : 0), 256);
   L.o_desc = off;   off = align_up(off + sizeof(ImgDesc) * (size_t)std::max(n, 1), 256);
   L.o_tmap = off;   off = align_up(off + sizeof(CUtensorMap) * 2 * (size_t)std::max(n, 1), 256);
   L.o_base = off;   off = align_up(off + 4ull * (n + 1), 256);
@@ -320,8 +323,24 @@ Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns) {
   const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * L.total + (1ull << 20));
   // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
   // this cap, which only turns a scheduling bug into an error instead of an endless run.
-  return Queue{reinterpret_cast<QueueHdr*>(dbase + L.o_hdr), reinterpret_cast<uint32_t*>(dbase + L.o_ring), L.cap - 1,
-               timeout_ns, (uint32_t)cap_visits, L.total};
+  Queue q{reinterpret_cast<QueueHdr*>(dbase + L.o_hdr), reinterpret_cast<uint32_t*>(dbase + L.o_ring), L.cap - 1,
+          timeout_ns, (uint32_t)cap_visits, L.total};
+  if (L.nb > 1) {
+    q.nb_mask = L.nb - 1;
+    q.keys = reinterpret_cast<uint32_t*>(dbase + L.o_keys);
+    q.wacc = reinterpret_cast<float*>(dbase + L.o_wacc);
+  }
+  return q;
+}
+
+dtb_status reset_queue(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, cudaStream_t stream) {
+  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_hdr, 0, sizeof(QueueHdr), stream));
+  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_ring, 0, L.ring_bytes(), stream));
+  if (L.nb > 1) {
+    DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_keys, 0xFF, 4ull * std::max<uint32_t>(L.total, 1), stream));  // KEY_NONE
+    DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_wacc, 0, 8ull * (size_t)std::max(L.n, 1), stream));
+  }
+  return DTB_OK;
 }
 
 dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
@@ -333,8 +352,8 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
   const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
   uint32_t* states = reinterpret_cast<uint32_t*>(dbase + L.o_states);
-  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_hdr, 0, sizeof(QueueHdr), stream));
-  DTB_CUDA(ctx, cudaMemsetAsync(dbase + L.o_ring, 0, 4ull * L.cap, stream));
+  dtb_status rs = reset_queue(ctx, dbase, L, stream);
+  if (rs != DTB_OK) return rs;
   if (L.total == 0) return DTB_OK;
   const int n = L.n;
   const uint32_t total = L.total;
@@ -369,7 +388,7 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
 // blocks variant (generalised_distance_transform_blocks.cu:156-163).
 static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, cudaStream_t stream,
                              uint64_t* nrounds) {
-  Queue q = make_queue(dbase, L);
+  Queue q = make_queue(dbase, L);  // rounds use only the counters and the error word of the queue
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + L.o_desc);
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
   const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
@@ -510,7 +529,8 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   LaunchTuning tuning = ctx->tuning;
   auto it = ctx->tuned.find(tuning_key(n, total));
   if (it != ctx->tuned.end()) tuning = it->second;
-  const ScratchLayout L = layout_for(n, total, resident_workers(ctx, mode, tuning), rounds);
+  const ScratchLayout L = layout_for(n, total, resident_workers(ctx, mode, tuning), rounds,
+                                     mode == MODE_NS && !rounds ? NBUCKET : 1u);
   if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, L.bytes)) != DTB_OK) return s;
   uint8_t* dbase = reinterpret_cast<uint8_t*>(ctx->dscratch);
   if ((s = build_tables(ctx, jobs, L, ctx->hstage)) != DTB_OK) return s;

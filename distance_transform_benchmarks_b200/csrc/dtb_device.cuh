@@ -64,10 +64,12 @@ struct alignas(64) ImgDesc {
 };
 
 // Counters live on separate 128-byte lines.
+constexpr uint32_t NBUCKET = 8;  // priority buckets of the tile queue (power of two; swept 8 < 16 < 32)
 struct alignas(128) Line { uint32_t v; uint32_t pad[31]; };
 struct QueueHdr {
-  Line head;       // next pop ticket
-  Line tail;       // next push position
+  Line heads[NBUCKET];  // next pop ticket, per bucket
+  Line tails[NBUCKET];  // next push position, per bucket
+  Line base;       // absolute index of the lowest bucket that may hold work (a hint: order is a heuristic)
   Line pending;    // tiles queued or running
   Line error;      // first device error code
   Line progress;   // completed visits (flushed per warp in batches; watchdog and visit cap)
@@ -77,14 +79,24 @@ struct QueueHdr {
   Line done;       // set once when pending reached 0
 };
 
+// The tile queue.  nb_mask = 0: one FIFO ring.  nb_mask = NBUCKET - 1: NBUCKET rings ordered by distance: an
+// activation carries the smallest value it can bring into the tile (a border distance plus an edge weight);
+// its bucket is that value in units of one tile-width of path cost of its image, relative to `base`.  Workers
+// take from the lowest non-empty bucket, which approximates visiting tiles in order of distance (Dijkstra
+// order on the tile graph) and so avoids most re-visits of tiles reached first by a costlier path.  The map
+// does not depend on the order: every order ends in the same fixpoint.
 struct Queue {
   QueueHdr* hdr;
-  uint32_t* ring;
+  uint32_t* ring;           // (nb_mask + 1) rings of (mask + 1) slots
   uint32_t mask;            // ring capacity - 1 (capacity is a power of two)
   uint64_t timeout_ns;      // watchdog: give up after this long without any completed visit
   uint32_t max_visits;      // safety net against endless re-activation
   uint32_t total_tiles;     // tile ids are < total_tiles
+  uint32_t nb_mask = 0;     // bucket count - 1
+  uint32_t* keys = nullptr;  // per tile: smallest pending activation value (float bits), KEY_NONE if none
+  float* wacc = nullptr;     // per image: [sum, count] of the internal edge weights seen by first visits
 };
+constexpr uint32_t KEY_NONE = 0xFFFFFFFFu;
 
 // Per-warp shared memory slot (13 KB: 16 warps per SM fit in 228 KB).
 constexpr int W_STRIDE = TILE + 1;  // weight / tile buffers: 33 floats per row, conflict-free in both layouts
@@ -155,63 +167,112 @@ __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
 // ------------------------------------------------------------------------------------------------------
 constexpr uint32_t SLOT_SENTINEL = 0xFFFFFFFFu;  // never an item: items are tile id + 1 < 2^31
 constexpr uint32_t POP_NONE = 0xFFFFFFFFu;
-constexpr uint64_t POLL_CHECK_NS = 20000;        // rare checks of done / error / watchdog while waiting
+constexpr uint64_t POLL_CHECK_NS = 2000;         // checks of done / error / watchdog / other buckets while waiting
 
 __device__ __forceinline__ void set_error(const Queue& q, uint32_t code, uint32_t info) {
   if (atomicCAS(&q.hdr->error.v, 0u, code) == 0u) atomicExch(&q.hdr->err_info.v, info);
 }
 
-// Writes item into ring position p once the slot is free (bounded wait).
-__device__ __forceinline__ void slot_write(const Queue& q, uint32_t p, uint32_t item) {
-  uint32_t* slot = &q.ring[p & q.mask];
-  if (atomicCAS(slot, 0u, item + 1u) == 0u) return;
+__device__ __forceinline__ uint32_t* ring_slot(const Queue& q, uint32_t b, uint32_t p) {
+  return &q.ring[(size_t)b * (q.mask + 1) + (p & q.mask)];
+}
+
+// A waiter that gave its ticket back marks its slot; the pusher that reaches the slot clears it and takes the
+// next position instead.  Never an item (items are tile id + 1 < 2^31) nor the sentinel.
+constexpr uint32_t SLOT_CANCELLED = 0xFFFFFFFEu;
+
+// Writes item into bucket b at position p once the slot is free (bounded wait); a cancelled slot is cleared and
+// the item goes to the next position of the bucket.
+__device__ __forceinline__ void slot_write(const Queue& q, uint32_t b, uint32_t p, uint32_t item) {
   uint32_t ns = 32;
   const uint64_t t0 = globaltimer();
-  while (atomicCAS(slot, 0u, item + 1u) != 0u) {
+  for (;;) {
+    uint32_t* slot = ring_slot(q, b, p);
+    const uint32_t prev = atomicCAS(slot, 0u, item + 1u);
+    if (prev == 0u) return;
+    if (prev == SLOT_CANCELLED) {
+      atomicCAS(slot, SLOT_CANCELLED, 0u);
+      p = atomicAdd(&q.hdr->tails[b].v, 1u);
+      continue;
+    }
     if (globaltimer() - t0 > q.timeout_ns) { set_error(q, DERR_RING_FULL, item); return; }
     __nanosleep(ns);
     ns = ns < 1024 ? ns * 2 : ns;
   }
 }
 
-// Single-item push (seed scan): pending += 1 before the item becomes visible.
-__device__ __forceinline__ void queue_push(const Queue& q, uint32_t item) {
+// Bucket of an activation value `key` (distance units) for an image whose bucket width is 1 / inv_width.
+// (Idle workers waiting in another bucket give their tickets back within POLL_CHECK_NS and find the item.)
+__device__ __forceinline__ uint32_t bucket_of(const Queue& q, float key, float inv_width) {
+  if (q.nb_mask == 0) return 0;
+  const uint32_t base = ld_volatile(&q.hdr->base.v);
+  const float r = key * inv_width;  // absolute bucket; NaN / huge values land in the last bucket
+  uint32_t rel = q.nb_mask;
+  if (r < 4.0e9f) {
+    const uint32_t kb = (uint32_t)r;
+    rel = kb <= base ? 0u : min(kb - base, q.nb_mask);
+  }
+  return (base + rel) & q.nb_mask;
+}
+
+// Pushes one item into bucket b: pending += 1 before the item becomes visible.
+__device__ __forceinline__ void queue_push_to(const Queue& q, uint32_t b, uint32_t item) {
   atomicAdd(&q.hdr->pending.v, 1u);
   __threadfence();
-  slot_write(q, atomicAdd(&q.hdr->tail.v, 1u), item);
+  slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
 }
 
-// Called by the whole warp of the visit that brought pending to 0.
+// Single-item push at the current base bucket (seed scans, warm starts).
+__device__ __forceinline__ void queue_push(const Queue& q, uint32_t item) {
+  queue_push_to(q, q.nb_mask ? (ld_volatile(&q.hdr->base.v) & q.nb_mask) : 0u, item);
+}
+
+// Called by the whole warp of the visit that brought pending to 0: wakes every popper waiting on a slot.
 __device__ __forceinline__ void signal_done_warp(const Queue& q) {
   const int lane = threadIdx.x & 31;
-  uint32_t h = 0, t = 0;
-  if (lane == 0) {
-    atomicExch(&q.hdr->done.v, 1u);
-    __threadfence();
-    h = ld_volatile(&q.hdr->head.v);
-    t = ld_volatile(&q.hdr->tail.v);
+  if (lane == 0) atomicExch(&q.hdr->done.v, 1u);
+  __threadfence();
+  for (uint32_t b = 0; b <= q.nb_mask; ++b) {
+    uint32_t h = 0, t = 0;
+    if (lane == 0) {
+      h = ld_volatile(&q.hdr->heads[b].v);
+      t = ld_volatile(&q.hdr->tails[b].v);
+    }
+    h = __shfl_sync(~0u, h, 0);
+    t = __shfl_sync(~0u, t, 0);
+    for (uint32_t p = t + (uint32_t)lane; (int32_t)(h - p) > 0; p += 32u)
+      *(volatile uint32_t*)ring_slot(q, b, p) = SLOT_SENTINEL;
   }
-  h = __shfl_sync(~0u, h, 0);
-  t = __shfl_sync(~0u, t, 0);
-  for (uint32_t p = t + (uint32_t)lane; (int32_t)(h - p) > 0; p += 32u)
-    *(volatile uint32_t*)&q.ring[p & q.mask] = SLOT_SENTINEL;
 }
 
-// Called by one lane.  Returns a tile id or POP_NONE (queue drained, or error).
-__device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
-  const uint32_t h = atomicAdd(&q.hdr->head.v, 1u);
-  __threadfence();  // the ticket before the checks below (pairs with the fence of signal_done_warp)
-  if (ld_volatile(&q.hdr->done.v) | ld_volatile(&q.hdr->error.v)) return POP_NONE;
-  if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;  // nothing queued at all
-  uint32_t* slot = &q.ring[h & q.mask];
+// Watchdog state of one popper, kept across the tickets it gives back.
+struct PopWatch {
+  uint64_t t_prog;
+  uint32_t seen;
+};
+
+constexpr uint32_t POP_RESCAN = 0xFFFFFFFDu;  // the ticket was given back: look for work elsewhere
+
+// Lowest bucket other than b with an item reserved and not taken (one lane, a few loads).
+__device__ __forceinline__ bool other_bucket_has_work(const Queue& q, uint32_t b) {
+  for (uint32_t i = 0; i <= q.nb_mask; ++i)
+    if (i != b && (int32_t)(ld_volatile(&q.hdr->tails[i].v) - ld_volatile(&q.hdr->heads[i].v)) > 0) return true;
+  return false;
+}
+
+// Waits for the item of ticket h of bucket b (one lane).  Bounded: done / error / pending / watchdog.  In the
+// bucketed queue a waiter whose item is not reserved yet gives the ticket back (POP_RESCAN) when another bucket
+// holds work, so idle workers never sit in a cold bucket while work waits elsewhere.
+__device__ __forceinline__ uint32_t slot_take(const Queue& q, uint32_t b, uint32_t h, PopWatch& w) {
+  uint32_t* slot = ring_slot(q, b, h);
   uint32_t ns = 32;
-  uint64_t t_check = globaltimer(), t_prog = t_check;
-  uint32_t seen = ld_volatile(&q.hdr->progress.v);
+  uint64_t t_check = globaltimer();
   for (;;) {
-    if (ld_volatile(slot) != 0u) {
+    const uint32_t cur = ld_volatile(slot);
+    if (cur != 0u && cur != SLOT_CANCELLED) {
       const uint32_t v = atomicExch(slot, 0u);
       if (v == SLOT_SENTINEL) return POP_NONE;
-      if (v != 0u) return v - 1u;
+      if (v != 0u && v != SLOT_CANCELLED) return v - 1u;
     }
     __nanosleep(ns);
     ns = ns < 256 ? ns * 2 : ns;
@@ -222,9 +283,51 @@ __device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
       if (ld_volatile(&q.hdr->pending.v) == 0u) return POP_NONE;
       const uint32_t prog = ld_volatile(&q.hdr->progress.v);
       if (prog > q.max_visits) { set_error(q, DERR_VISIT_LIMIT, prog); return POP_NONE; }
-      if (prog != seen) { seen = prog; t_prog = now; }
-      else if (now - t_prog > q.timeout_ns) { set_error(q, DERR_QUEUE_TIMEOUT, h); return POP_NONE; }
+      if (prog != w.seen) { w.seen = prog; w.t_prog = now; }
+      else if (now - w.t_prog > q.timeout_ns) { set_error(q, DERR_QUEUE_TIMEOUT, h); return POP_NONE; }
+      if (q.nb_mask && (int32_t)(ld_volatile(&q.hdr->tails[b].v) - h) <= 0 && other_bucket_has_work(q, b)) {
+        if (atomicCAS(slot, 0u, SLOT_CANCELLED) == 0u) return POP_RESCAN;
+      }
     }
+  }
+}
+
+// Pop, called by the whole warp; every lane gets the tile id or POP_NONE (queue drained, or error).
+// FIFO: a ticket, then the popper waits on its own slot only (no shared hot line is polled).
+// Bucketed: one load per bucket across the lanes finds the lowest bucket with work and the ticket is taken
+// there; with no work anywhere the ticket is taken in the base bucket, whose pushes feed waiting poppers
+// first.  Either way the popper then waits on its own slot.
+__device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
+  const int lane = threadIdx.x & 31;
+  PopWatch w{globaltimer(), 0u};
+  if (lane == 0) w.seen = ld_volatile(&q.hdr->progress.v);
+  for (;;) {
+    uint32_t base = 0, m = 0;
+    if (q.nb_mask) {
+      if (lane == 0) base = ld_volatile(&q.hdr->base.v);
+      base = __shfl_sync(~0u, base, 0);
+      const uint32_t bl = (base + (uint32_t)lane) & q.nb_mask;
+      bool avail = false;
+      if ((uint32_t)lane <= q.nb_mask)
+        avail = (int32_t)(ld_volatile(&q.hdr->tails[bl].v) - ld_volatile(&q.hdr->heads[bl].v)) > 0;
+      m = __ballot_sync(~0u, avail);
+    }
+    uint32_t res = POP_NONE;
+    if (lane == 0) {
+      uint32_t b = base & q.nb_mask;
+      if (m) {
+        const uint32_t f = (uint32_t)(__ffs(m) - 1);
+        if (f > 0) atomicCAS(&q.hdr->base.v, base, base + f);  // the lower buckets are empty: move the hint up
+        b = (base + f) & q.nb_mask;
+      }
+      const uint32_t h = atomicAdd(&q.hdr->heads[b].v, 1u);
+      __threadfence();  // the ticket before the checks below (pairs with the fence of signal_done_warp)
+      if (ld_volatile(&q.hdr->done.v) | ld_volatile(&q.hdr->error.v)) res = POP_NONE;
+      else if (ld_volatile(&q.hdr->pending.v) == 0u) res = POP_NONE;  // nothing queued at all
+      else res = slot_take(q, b, h, w);
+    }
+    res = __shfl_sync(~0u, res, 0);
+    if (res != POP_RESCAN) return res;
   }
 }
 

@@ -69,8 +69,11 @@ inline float gamma_to_g2(float gamma) {
 struct ScratchLayout {
   int n = 0;
   uint32_t total = 0;  // tiles
-  uint32_t cap = 0;    // ring slots (power of two)
-  size_t o_hdr = 0, o_states = 0, o_ring = 0, o_desc = 0, o_tmap = 0, o_base = 0, o_act = 0, o_chg = 0, bytes = 0;
+  uint32_t cap = 0;    // ring slots per bucket (power of two)
+  uint32_t nb = 1;     // priority buckets of the tile queue (1 or NBUCKET)
+  size_t o_hdr = 0, o_states = 0, o_ring = 0, o_keys = 0, o_wacc = 0, o_desc = 0, o_tmap = 0, o_base = 0, o_act = 0,
+         o_chg = 0, bytes = 0;
+  size_t ring_bytes() const { return 4ull * cap * nb; }
 };
 
 // Launch parameters of the tile kernel chosen for a run.
@@ -130,8 +133,11 @@ dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name,
 // Checks that img / mask / dist form one image of the given kinds (rgb allowed or not).
 dtb_status check_triplet(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist, bool allow_rgb);
 
-// Scratch layout for n images with `total` tiles, `workers` resident warps; `rounds` adds the round flags.
-ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds);
+// Scratch layout for n images with `total` tiles, `workers` resident warps; `rounds` adds the round flags;
+// `buckets`: priority buckets of the tile queue (NBUCKET for ns-mode runs, 1 = one FIFO ring).
+ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, uint32_t buckets = NBUCKET);
+// Enqueues the reset of the queue part of a scratch block (header, rings, activation keys, bucket widths).
+dtb_status reset_queue(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, cudaStream_t stream);
 // Host image of [descriptors | tensor maps | tile prefix] (bytes o_desc .. o_act of the layout).
 dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const ScratchLayout& L, std::vector<uint8_t>& out);
 // Total tiles of the jobs (error if beyond the 31-bit tile id space).

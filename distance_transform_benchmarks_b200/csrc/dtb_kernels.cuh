@@ -18,6 +18,7 @@
 namespace dtb {
 
 constexpr int PHASE_LIMIT = 4096;
+constexpr float BUCKET_TILES = 0.5f;  // priority bucket width, in tile-widths of path cost (swept: 0.5 < 1 < 2)
 constexpr uint64_t TMA_TIMEOUT_NS = 2000000000ull;  // 2 s
 
 // ------------------------------------------------------------------------------------------------------
@@ -31,19 +32,26 @@ struct WarpStats {
 struct QueueSched {
   Queue q;
   uint32_t* states;
-  // Warp-level end of a visit.  Lanes with `want` ask for a re-run of neighbour `item`: idle -> queued;
-  // running -> running with a re-run requested; queued -> unchanged.  Lane 31 clears RUNNING of the own
-  // tile (and sets / clears the xor_bits); a re-run requested meanwhile re-queues it.  `pending` moves by
-  // (pushes - 1) in one atomic performed before any push is visible; the visit that brings it to 0 ends
-  // the queue.
-  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item) const {
+  // Warp-level end of a visit.  Lanes with `want` ask for a re-run of neighbour `item`, bringing activation
+  // value `key` (distance units; bucket width 1 / inv_width): idle -> queued; running -> running with a re-run
+  // requested; queued -> unchanged.  Lane 31 clears RUNNING of the own tile (and sets / clears the xor_bits);
+  // a re-run requested meanwhile re-queues it at the smallest value its activators left in keys[].  `pending`
+  // moves by (pushes - 1) in one atomic performed before any push is visible; the visit that brings it to 0
+  // ends the queue.
+  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item,
+                                           float key = 0.0f, float inv_width = 0.0f) const {
     const int lane = threadIdx.x & 31;
     bool push = false;
     uint32_t item = 0;
+    float pkey = key;
     if (want) {
       if (want_item >= q.total_tiles) {
         set_error(q, DERR_BAD_TILE, want_item);
       } else {
+        if (q.keys) {
+          const uint32_t prev = atomicMin(&q.keys[want_item], __float_as_uint(key));
+          pkey = fminf(key, __uint_as_float(prev == KEY_NONE ? __float_as_uint(key) : prev));
+        }
         const uint32_t old = atomicOr(&states[want_item], ST_PENDING);
         push = !(old & (ST_PENDING | ST_RUNNING));
         item = want_item;
@@ -53,24 +61,27 @@ struct QueueSched {
       const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
       push = (old & ST_PENDING) != 0u;
       item = tile;
+      if (push && q.keys) {
+        const uint32_t kb = ld_volatile(&q.keys[tile]);
+        pkey = kb == KEY_NONE ? 0.0f : __uint_as_float(kb);
+      }
     }
     const uint32_t m = __ballot_sync(~0u, push);
     const uint32_t k = __popc(m);
-    uint32_t base = 0, last = 0;
+    uint32_t last = 0;
     if (lane == 0) {
       if (k == 0) {
         last = atomicSub(&q.hdr->pending.v, 1u) == 1u ? 1u : 0u;
-      } else {
-        if (k > 1) {
-          atomicAdd(&q.hdr->pending.v, k - 1u);
-          __threadfence();
-        }
-        base = atomicAdd(&q.hdr->tail.v, k);
+      } else if (k > 1) {
+        atomicAdd(&q.hdr->pending.v, k - 1u);
       }
+      __threadfence();
     }
     __syncwarp();
-    base = __shfl_sync(~0u, base, 0);
-    if (push) slot_write(q, base + __popc(m & ((1u << lane) - 1u)), item);
+    if (push) {
+      const uint32_t b = bucket_of(q, pkey, inv_width);
+      slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
+    }
     if (__shfl_sync(~0u, last, 0)) signal_done_warp(q);
   }
 };
@@ -80,7 +91,8 @@ struct RoundSched {
   uint32_t* states;
   uint8_t* next_active;
   uint32_t* changed;
-  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item) const {
+  __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item,
+                                           float = 0.0f, float = 0.0f) const {
     if (want) {
       if (want_item >= q.total_tiles) {
         set_error(q, DERR_BAD_TILE, want_item);
@@ -302,6 +314,33 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   }
   __syncwarp();
 
+  // Bucket width of this image: one tile-width of path cost, 32 x the mean internal edge weight seen so far by
+  // first visits (each first visit adds its column edges).
+  const uint32_t img_idx = old_state >> ST_IMG_SHIFT;
+  float inv_width = 0.0f;
+  if (sch.q.wacc) {
+    float* wa = sch.q.wacc + 2 * img_idx;
+    if (first) {
+      float wsum = 0.0f, wcnt = 0.0f;
+#pragma unroll 4
+      for (int y = 1; y < TILE; ++y) {
+        const float w = sm.Wv[y * W_STRIDE + lane];
+        if (w < INF) { wsum += w; wcnt += 1.0f; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        wsum += __shfl_xor_sync(~0u, wsum, o);
+        wcnt += __shfl_xor_sync(~0u, wcnt, o);
+      }
+      if (lane == 0 && wcnt > 0.0f) {
+        atomicAdd(&wa[0], wsum);
+        atomicAdd(&wa[1], wcnt);
+      }
+    }
+    const float s_ = *(volatile float*)&wa[0], c_ = *(volatile float*)&wa[1];
+    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (BUCKET_TILES * (float)TILE * s_) : 1.0f / (BUCKET_TILES * (float)TILE);
+  }
+
   // Local fixpoint.  B overlays the image box, which is no longer needed.
   float* B = reinterpret_cast<float*>(sm.img);
   // Start in the layout whose chains begin at the halo sides that can lower the tile now: a column phase
@@ -378,17 +417,23 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 
   // Neighbours that can still decrease (bit 0 left, 1 right, 2 top, 3 bottom).
   uint32_t act = 0;
+  float act_key = 0.0f;
   if (any || seed) {
     const float dt = B[lane], db = B[(TILE - 1) * W_STRIDE + lane];               // column layout
     const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];      // row layout
     const float wt = sm.Wv[lane], wb = sm.Wv[TILE * W_STRIDE + lane];
     const float wl = sm.Wh[lane * W_STRIDE], wr = sm.Wh[lane * W_STRIDE + TILE];
-    act |= __any_sync(~0u, __fadd_rn(dl, wl) < lft) ? 1u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dr, wr) < rgt) ? 2u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(dt, wt) < top) ? 4u : 0u;
-    act |= __any_sync(~0u, __fadd_rn(db, wb) < bot) ? 8u : 0u;
+    // The activation value of a side: the smallest border value it can bring (its priority in the queue).
+    const float vl = __fadd_rn(dl, wl), vr = __fadd_rn(dr, wr), vt = __fadd_rn(dt, wt), vb = __fadd_rn(db, wb);
+    const uint32_t kl = __reduce_min_sync(~0u, vl < lft ? __float_as_uint(vl) : KEY_NONE);
+    const uint32_t kr = __reduce_min_sync(~0u, vr < rgt ? __float_as_uint(vr) : KEY_NONE);
+    const uint32_t kt = __reduce_min_sync(~0u, vt < top ? __float_as_uint(vt) : KEY_NONE);
+    const uint32_t kbm = __reduce_min_sync(~0u, vb < bot ? __float_as_uint(vb) : KEY_NONE);
+    act = (kl != KEY_NONE ? 1u : 0u) | (kr != KEY_NONE ? 2u : 0u) | (kt != KEY_NONE ? 4u : 0u) |
+          (kbm != KEY_NONE ? 8u : 0u);
     // A missing neighbour has an INF halo, and fl(d + w) < INF holds for any finite d: mask by existence.
     act &= nexist;
+    act_key = __uint_as_float(lane == 0 ? kl : lane == 1 ? kr : lane == 2 ? kt : kbm);
   }
 
   // Write back (column layout: each row is one coalesced 128-byte store).
@@ -401,7 +446,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   }
   __threadfence();  // release: distances before activations and before the VISITED bit
   __syncwarp();
-  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), lane < 4 && ((act >> lane) & 1u), nb_tile);
+  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), lane < 4 && ((act >> lane) & 1u), nb_tile,
+               act_key, inv_width);
   *nph_out = nph;
   *nact_out = (uint32_t)__popc(act);
 }

@@ -96,13 +96,10 @@ __global__ void __launch_bounds__(NOALLOC_WPC * 32, NOALLOC_MINB) noalloc_persis
   uint32_t parity = 0;
   WarpStats ws;
   for (;;) {
-    uint32_t t = POP_NONE, old = 0;
-    if (lane == 0) {
-      t = queue_pop(q);
-      if (t != POP_NONE) old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
-    }
-    t = __shfl_sync(~0u, t, 0);
+    const uint32_t t = queue_pop(q);  // one FIFO ring: this scratch holds no priority buckets
     if (t == POP_NONE) break;
+    uint32_t old = 0;
+    if (lane == 0) old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
     old = __shfl_sync(~0u, old, 0);
     const ImgDesc dd = *na_desc();
     visit_tile<MODE_NS>(dd, na_tmaps(), 0u, t, old, sm, parity, sch, ws);

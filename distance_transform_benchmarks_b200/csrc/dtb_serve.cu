@@ -399,8 +399,8 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
   std::copy(reinterpret_cast<const uint8_t*>(items.data()), reinterpret_cast<const uint8_t*>(items.data() + items.size()),
             s->host.begin() + (o_items - L.o_desc));
   DTB_CUDA(ctx, cudaMemcpyAsync(sc + L.o_desc, s->host.data(), s->host.size(), cudaMemcpyHostToDevice, st));
-  DTB_CUDA(ctx, cudaMemsetAsync(sc + L.o_hdr, 0, sizeof(QueueHdr), st));
-  DTB_CUDA(ctx, cudaMemsetAsync(sc + L.o_ring, 0, 4ull * L.cap, st));
+  const dtb_status qs = reset_queue(ctx, sc, L, st);
+  if (qs != DTB_OK) return qs;
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(sc + L.o_desc);
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(sc + L.o_tmap);
   const uint32_t* dbase = reinterpret_cast<const uint32_t*>(sc + L.o_base);
