@@ -315,6 +315,28 @@ dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const Scr
   return DTB_OK;
 }
 
+dtb_status pinned_stage(dtb_context ctx, size_t need, uint8_t** out, cudaEvent_t* ev) {
+  const int i = ctx->hpin_cur;
+  ctx->hpin_cur ^= 1;
+  if (!ctx->hpin_ev[i]) DTB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->hpin_ev[i], cudaEventDisableTiming));
+  if (ctx->hpin_used[i]) DTB_CUDA(ctx, cudaEventSynchronize(ctx->hpin_ev[i]));
+  if (ctx->hpin_size[i] < need) {
+    if (ctx->hpin[i]) cudaFreeHost(ctx->hpin[i]);
+    ctx->hpin[i] = nullptr;
+    ctx->hpin_size[i] = 0;
+    const size_t sz = std::max<size_t>(need + need / 4, 1 << 20);
+    if (cudaHostAlloc(&ctx->hpin[i], sz, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "cudaHostAlloc of %zu bytes failed", sz);
+    }
+    ctx->hpin_size[i] = sz;
+  }
+  ctx->hpin_used[i] = true;
+  *out = static_cast<uint8_t*>(ctx->hpin[i]);
+  *ev = ctx->hpin_ev[i];
+  return DTB_OK;
+}
+
 uint64_t tuning_key(int n, uint32_t total) {
   return ((uint64_t)next_pow2((uint32_t)std::max(n, 1)) << 32) | next_pow2(std::max<uint32_t>(total, 1));
 }
@@ -530,11 +552,18 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   auto it = ctx->tuned.find(tuning_key(n, total));
   if (it != ctx->tuned.end()) tuning = it->second;
   const ScratchLayout L = layout_for(n, total, resident_workers(ctx, mode, tuning), rounds,
-                                     mode == MODE_NS && !rounds ? NBUCKET : 1u);
+                                     rounds ? 1u : NBUCKET);
   if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, L.bytes)) != DTB_OK) return s;
   uint8_t* dbase = reinterpret_cast<uint8_t*>(ctx->dscratch);
   if ((s = build_tables(ctx, jobs, L, ctx->hstage)) != DTB_OK) return s;
-  DTB_CUDA(ctx, cudaMemcpyAsync(dbase + L.o_desc, ctx->hstage.data(), ctx->hstage.size(), cudaMemcpyHostToDevice, stream));
+  {  // from pinned memory: the copy never waits for earlier work on the stream
+    uint8_t* hp = nullptr;
+    cudaEvent_t ev_host = nullptr;
+    if ((s = pinned_stage(ctx, ctx->hstage.size(), &hp, &ev_host)) != DTB_OK) return s;
+    std::copy(ctx->hstage.begin(), ctx->hstage.end(), hp);
+    DTB_CUDA(ctx, cudaMemcpyAsync(dbase + L.o_desc, hp, ctx->hstage.size(), cudaMemcpyHostToDevice, stream));
+    DTB_CUDA(ctx, cudaEventRecord(ev_host, stream));
+  }
 
   uint64_t nrounds = 1;
   const bool timed = (flags & DTB_FLAG_TIMING) && !rounds && total > 0;
@@ -673,6 +702,10 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
   if (ctx->dscratch) cudaFree(ctx->dscratch);
   if (ctx->dround_counts) cudaFree(ctx->dround_counts);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->hpin[i]) cudaFreeHost(ctx->hpin[i]);
+    if (ctx->hpin_ev[i]) cudaEventDestroy(ctx->hpin_ev[i]);
+  }
   if (ctx->dstage) cudaFree(ctx->dstage);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);

@@ -226,18 +226,33 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   }
   if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, soff)) != DTB_OK) return s;
   uint8_t* scratch = static_cast<uint8_t*>(ctx->dscratch);
-  std::vector<uint8_t>& host = ctx->hstage;
-  host.assign(soff, 0);
+  // Only the descriptor tables, tensor maps and repitch lists of each chunk go up (one pinned block, one copy
+  // per part); queue headers, rings and tile states are reset on the device by each chunk's run.
+  size_t hbytes = 0;
+  std::vector<size_t> h_tab(nchunks), h_items(nchunks);
+  for (int k = 0; k < nchunks; ++k) {
+    h_tab[k] = hbytes;
+    hbytes += L[k].o_act - L[k].o_desc;
+    h_items[k] = hbytes;
+    hbytes += sizeof(RepitchItem) * items[k].size();
+  }
+  uint8_t* host = nullptr;
+  cudaEvent_t ev_host = nullptr;
+  if ((s = pinned_stage(ctx, hbytes, &host, &ev_host)) != DTB_OK) return s;
   for (int k = 0; k < nchunks; ++k) {
     std::vector<Job> cj(jobs.begin() + cut[k], jobs.begin() + cut[k + 1]);
-    std::vector<uint8_t> tab;
+    std::vector<uint8_t>& tab = ctx->hstage;
     if ((s = build_tables(ctx, cj, L[k], tab)) != DTB_OK) return s;
-    std::copy(tab.begin(), tab.end(), host.begin() + o_chunk[k] + L[k].o_desc);
+    std::copy(tab.begin(), tab.end(), host + h_tab[k]);
     std::copy(reinterpret_cast<const uint8_t*>(items[k].data()),
-              reinterpret_cast<const uint8_t*>(items[k].data() + items[k].size()), host.begin() + o_items[k]);
+              reinterpret_cast<const uint8_t*>(items[k].data() + items[k].size()), host + h_items[k]);
+    DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_chunk[k] + L[k].o_desc, host + h_tab[k], tab.size(), cudaMemcpyHostToDevice,
+                                  stream));
+    if (!items[k].empty())
+      DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_items[k], host + h_items[k], sizeof(RepitchItem) * items[k].size(),
+                                    cudaMemcpyHostToDevice, stream));
   }
-  // Pageable source: the copy has consumed it when the call returns.
-  DTB_CUDA(ctx, cudaMemcpyAsync(scratch, host.data(), soff, cudaMemcpyHostToDevice, stream));
+  DTB_CUDA(ctx, cudaEventRecord(ev_host, stream));
   cudaEvent_t ev_tables = event_at(ctx, 0);
   if (!ev_tables) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
   DTB_CUDA(ctx, cudaEventRecord(ev_tables, stream));

@@ -106,6 +106,13 @@ struct dtb_context_s {
   bool async_pending = false;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // DTB_FLAG_TIMING: around the tile kernel
   bool timed = false;
+  // Pinned host staging of descriptor tables, double-buffered: buffer i may be refilled once event i (recorded
+  // after the copies out of it) has completed.
+  void* hpin[2] = {nullptr, nullptr};
+  size_t hpin_size[2] = {0, 0};
+  cudaEvent_t hpin_ev[2] = {nullptr, nullptr};
+  bool hpin_used[2] = {false, false};
+  int hpin_cur = 0;
   // Host-buffer pipeline: copy streams, a second compute lane, events, chunk size in pixels.
   cudaStream_t s_in = nullptr, s_out = nullptr, s_lane = nullptr;
   std::vector<cudaEvent_t> evpool;
@@ -155,6 +162,9 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_ima
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
                              const dtb_image* const* masks, const dtb_image* const* dists, cudaStream_t stream);
 dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need);
+// Next pinned table-staging buffer of at least `need` bytes (waits until its previous copies are done);
+// *ev is to be recorded after the copies out of it.
+dtb_status pinned_stage(dtb_context ctx, size_t need, uint8_t** out, cudaEvent_t* ev);
 
 // Kernels shared across translation units (defined in dtb_api.cu / dtb_host_pipeline.cu).
 __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,

@@ -456,9 +456,9 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 // ref-mode visit (C8, reference weight), gray only.
 //
 // Mirrors the reference's in-tile passes (dt/src/dt_block_passes.cuh:12-127): a row phase relaxes every
-// pixel from its three predecessors in the previous column (forward then backward), a column phase from
-// the three predecessors in the previous row.  The three rows (columns) move in lockstep, so the
-// predecessors of lane l come from lanes l-1 / l+1 by shuffle, or from the halo for the edge lanes.
+// pixel from its three predecessors in the previous column (forward and backward chains interleaved), a
+// column phase from the three predecessors in the previous row.  The three rows (columns) move in lockstep,
+// so the predecessors of lane l come from lanes l-1 / l+1 by shuffle, or from the halo for the edge lanes.
 // Each relaxation is a single edge with the reference's arithmetic (ref_relax).  Neighbours (8 of them)
 // are re-activated when a border pixel facing them decreased, as in dt_block_passes.cuh:50-63, and on
 // visits that applied seeds.
@@ -577,90 +577,127 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   };
   auto absd = [](float a, float b) { return fabsf(a - b); };  // exact for integers in [0, 255]
 
+  // Bucket width of this image (priority queue): half a tile-width of the mean axial edge cost
+  // l_eucl + l_grad * |dI| seen by first visits (vertical edges of the tile).
+  float inv_width = 0.0f;
+  if (sch.q.wacc) {
+    float* wa = sch.q.wacc + 2 * (old_state >> ST_IMG_SHIFT);
+    if (first) {
+      float wsum = 0.0f, wcnt = 0.0f;
+      if (lane < vw) {
+#pragma unroll 1
+        for (int y = 1; y < vh; ++y) {
+          wsum += le + lg * absd(P(y, lane), P(y - 1, lane));
+          wcnt += 1.0f;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        wsum += __shfl_xor_sync(~0u, wsum, o);
+        wcnt += __shfl_xor_sync(~0u, wcnt, o);
+      }
+      if (lane == 0 && wcnt > 0.0f) {
+        atomicAdd(&wa[0], wsum);
+        atomicAdd(&wa[1], wcnt);
+      }
+    }
+    const float s_ = *(volatile float*)&wa[0], c_ = *(volatile float*)&wa[1];
+    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (BUCKET_TILES * (float)TILE * s_) : 1.0f / (BUCKET_TILES * (float)TILE);
+  }
+
   bool any = false;
   uint32_t nph = 0;
   bool col = true;
   for (;;) {
     bool ch = false;
+    // The forward and the backward chain of the phase are interleaved (two independent dependency chains per
+    // warp); every step is the same single-edge relaxation as in the reference passes, so the order does not
+    // change the fixpoint.
     if (col) {
-      // Column phase (lane = x): forward over y with predecessors (x-1..x+1, y-1), then backward.
+      // Column phase (lane = x): forward over y with predecessors (x-1..x+1, y-1), backward with (x-1..x+1, y+1).
       const int x = lane;
       const bool xin = lane < vw;
 #pragma unroll
-      for (int y = 0; y < TILE; ++y) {
-        float pa, pb, pc;
-        if (y == 0) { pa = ht[x]; pb = ht[x + 1]; pc = ht[x + 2]; }
-        else {
-          pb = d[y - 1];
-          pa = __shfl_up_sync(~0u, pb, 1);
-          pc = __shfl_down_sync(~0u, pb, 1);
-          if (lane == 0) pa = hl[y];
-          if (lane == TILE - 1) pc = hr[y];
+      for (int k = 0; k < TILE; ++k) {
+        {
+          const int y = k;
+          float pa, pb, pc;
+          if (y == 0) { pa = ht[x]; pb = ht[x + 1]; pc = ht[x + 2]; }
+          else {
+            pb = d[y - 1];
+            pa = __shfl_up_sync(~0u, pb, 1);
+            pc = __shfl_down_sync(~0u, pb, 1);
+            if (lane == 0) pa = hl[y];
+            if (lane == TILE - 1) pc = hr[y];
+          }
+          const float c = P(y, x);
+          const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y - 1, x)),
+                                         absd(c, P(y - 1, x + 1)), true, true);
+          const bool upd = xin && y < vh && nd < d[y];
+          ch |= upd;
+          d[y] = upd ? nd : d[y];
         }
-        const float c = P(y, x);
-        const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y - 1, x)),
-                                       absd(c, P(y - 1, x + 1)), true, true);
-        const bool upd = xin && y < vh && nd < d[y];
-        ch |= upd;
-        d[y] = upd ? nd : d[y];
-      }
-#pragma unroll
-      for (int y = TILE - 1; y >= 0; --y) {
-        float pa, pb, pc;
-        if (y == TILE - 1) { pa = hb[x]; pb = hb[x + 1]; pc = hb[x + 2]; }
-        else {
-          pb = d[y + 1];
-          pa = __shfl_up_sync(~0u, pb, 1);
-          pc = __shfl_down_sync(~0u, pb, 1);
-          if (lane == 0) pa = hl[y + 2];
-          if (lane == TILE - 1) pc = hr[y + 2];
+        {
+          const int y = TILE - 1 - k;
+          float pa, pb, pc;
+          if (y == TILE - 1) { pa = hb[x]; pb = hb[x + 1]; pc = hb[x + 2]; }
+          else {
+            pb = d[y + 1];
+            pa = __shfl_up_sync(~0u, pb, 1);
+            pc = __shfl_down_sync(~0u, pb, 1);
+            if (lane == 0) pa = hl[y + 2];
+            if (lane == TILE - 1) pc = hr[y + 2];
+          }
+          const float c = P(y, x);
+          const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y + 1, x - 1)), absd(c, P(y + 1, x)),
+                                         absd(c, P(y + 1, x + 1)), true, true);
+          const bool upd = xin && y < vh && nd < d[y];
+          ch |= upd;
+          d[y] = upd ? nd : d[y];
         }
-        const float c = P(y, x);
-        const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y + 1, x - 1)), absd(c, P(y + 1, x)),
-                                       absd(c, P(y + 1, x + 1)), true, true);
-        const bool upd = xin && y < vh && nd < d[y];
-        ch |= upd;
-        d[y] = upd ? nd : d[y];
       }
     } else {
-      // Row phase (lane = y): forward over x with predecessors (x-1, y-1..y+1), then backward.
+      // Row phase (lane = y): forward over x with predecessors (x-1, y-1..y+1), backward with (x+1, y-1..y+1).
       const int y = lane;
       const bool yin = lane < vh;
 #pragma unroll
-      for (int x = 0; x < TILE; ++x) {
-        float pa, pb, pc;
-        if (x == 0) { pa = hl[y]; pb = hl[y + 1]; pc = hl[y + 2]; }
-        else {
-          pb = d[x - 1];
-          pa = __shfl_up_sync(~0u, pb, 1);
-          pc = __shfl_down_sync(~0u, pb, 1);
-          if (lane == 0) pa = ht[x];
-          if (lane == TILE - 1) pc = hb[x];
+      for (int k = 0; k < TILE; ++k) {
+        {
+          const int x = k;
+          float pa, pb, pc;
+          if (x == 0) { pa = hl[y]; pb = hl[y + 1]; pc = hl[y + 2]; }
+          else {
+            pb = d[x - 1];
+            pa = __shfl_up_sync(~0u, pb, 1);
+            pc = __shfl_down_sync(~0u, pb, 1);
+            if (lane == 0) pa = ht[x];
+            if (lane == TILE - 1) pc = hb[x];
+          }
+          const float c = P(y, x);
+          const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y, x - 1)),
+                                         absd(c, P(y + 1, x - 1)), true, true);
+          const bool upd = yin && x < vw && nd < d[x];
+          ch |= upd;
+          d[x] = upd ? nd : d[x];
         }
-        const float c = P(y, x);
-        const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y, x - 1)),
-                                       absd(c, P(y + 1, x - 1)), true, true);
-        const bool upd = yin && x < vw && nd < d[x];
-        ch |= upd;
-        d[x] = upd ? nd : d[x];
-      }
-#pragma unroll
-      for (int x = TILE - 1; x >= 0; --x) {
-        float pa, pb, pc;
-        if (x == TILE - 1) { pa = hr[y]; pb = hr[y + 1]; pc = hr[y + 2]; }
-        else {
-          pb = d[x + 1];
-          pa = __shfl_up_sync(~0u, pb, 1);
-          pc = __shfl_down_sync(~0u, pb, 1);
-          if (lane == 0) pa = ht[x + 2];
-          if (lane == TILE - 1) pc = hb[x + 2];
+        {
+          const int x = TILE - 1 - k;
+          float pa, pb, pc;
+          if (x == TILE - 1) { pa = hr[y]; pb = hr[y + 1]; pc = hr[y + 2]; }
+          else {
+            pb = d[x + 1];
+            pa = __shfl_up_sync(~0u, pb, 1);
+            pc = __shfl_down_sync(~0u, pb, 1);
+            if (lane == 0) pa = ht[x + 2];
+            if (lane == TILE - 1) pc = hb[x + 2];
+          }
+          const float c = P(y, x);
+          const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x + 1)), absd(c, P(y, x + 1)),
+                                         absd(c, P(y + 1, x + 1)), true, true);
+          const bool upd = yin && x < vw && nd < d[x];
+          ch |= upd;
+          d[x] = upd ? nd : d[x];
         }
-        const float c = P(y, x);
-        const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x + 1)), absd(c, P(y, x + 1)),
-                                       absd(c, P(y + 1, x + 1)), true, true);
-        const bool upd = yin && x < vw && nd < d[x];
-        ch |= upd;
-        d[x] = upd ? nd : d[x];
       }
     }
     ch = __any_sync(~0u, ch);
@@ -687,14 +724,21 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   }
   if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);
 
-  // Border changes -> neighbours (bit k = neighbour k as in ndx/ndy).
+  // Border changes -> neighbours (bit k = neighbour k as in ndx/ndy), as the reference activates blocks
+  // (dt_block_passes.cuh:50-63).  An exact "can this border lower the neighbour's halo" test (as in ns-mode)
+  // removed only a tenth of the visits here and cost more than it saved: most re-visits in ref-mode carry
+  // last-bit improvements of equally long paths summed in another order, which that test also lets through.
+  // The activation's priority is the smallest border value facing the neighbour.
   uint32_t act = 0;
+  float key = 0.0f;
   if (any || seed) {
     const bool force = seed;
-    const uint32_t ct = __ballot_sync(~0u, force || T[lane] != it0);
-    const uint32_t cb = __ballot_sync(~0u, force || T[(TILE - 1) * S_STRIDE + lane] != ib0);
-    const uint32_t cl = __ballot_sync(~0u, force || T[lane * S_STRIDE] != il0);
-    const uint32_t cr = __ballot_sync(~0u, force || T[lane * S_STRIDE + TILE - 1] != ir0);
+    const float bt = T[lane], bb = T[(TILE - 1) * S_STRIDE + lane];
+    const float bl = T[lane * S_STRIDE], br = T[lane * S_STRIDE + TILE - 1];
+    const uint32_t ct = __ballot_sync(~0u, force || bt != it0);
+    const uint32_t cb = __ballot_sync(~0u, force || bb != ib0);
+    const uint32_t cl = __ballot_sync(~0u, force || bl != il0);
+    const uint32_t cr = __ballot_sync(~0u, force || br != ir0);
     act |= cl ? 1u : 0u;
     act |= cr ? 2u : 0u;
     act |= ct ? 4u : 0u;
@@ -704,6 +748,16 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
     act |= (cb & 1u) ? 64u : 0u;
     act |= (cb >> (TILE - 1)) & 1u ? 128u : 0u;
     act &= nexist;
+    if (act) {
+      const uint32_t kl = __reduce_min_sync(~0u, __float_as_uint(bl));
+      const uint32_t kr = __reduce_min_sync(~0u, __float_as_uint(br));
+      const uint32_t kt = __reduce_min_sync(~0u, __float_as_uint(bt));
+      const uint32_t kb = __reduce_min_sync(~0u, __float_as_uint(bb));
+      const float corner = lane == 4 ? T[0] : lane == 5 ? T[TILE - 1] : lane == 6 ? T[(TILE - 1) * S_STRIDE]
+                                                                                    : T[(TILE - 1) * S_STRIDE + TILE - 1];
+      key = lane == 0 ? __uint_as_float(kl) : lane == 1 ? __uint_as_float(kr) : lane == 2 ? __uint_as_float(kt)
+          : lane == 3 ? __uint_as_float(kb) : corner;
+    }
   }
 
   if (any || first) {
@@ -717,7 +771,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   __syncwarp();
   const bool want = lane < 8 && ((act >> lane) & 1u);
   const uint32_t item = want ? dd.tile_base + (uint32_t)((ty + ndy[lane]) * dd.tiles_x + tx + ndx[lane]) : 0u;
-  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), want, item);
+  sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), want, item, key, inv_width);
   *nph_out = nph;
   *nact_out = (uint32_t)__popc(act);
 }
