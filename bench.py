@@ -386,16 +386,20 @@ def run_ours(args, dist):
         d2h = sum(t.numel() * t.element_size() for t in hdists)
 
         def estep():
-            dtb.geodesic_distance_transform_batch(himgs, hmasks, gammas, dists=hdists, ctx=ctx, stream=stream)
+            # Asynchronous call: the next step's host-side preparation overlaps this step's copies and runs.
+            dtb.geodesic_distance_transform_batch(himgs, hmasks, gammas, dists=hdists, ctx=ctx, stream=stream,
+                                                  asynchronous=True)
 
         for _ in range(2):
             estep()
+        ctx.sync(stream)
         dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(args.steps):
             estep()
         e1.record(stream)
+        ctx.sync(stream)  # raises on a device error of any step
         torch.cuda.synchronize()
         ems = dist.max(e0.elapsed_time(e1) / args.steps, "cuda")
         e2e = {"value": px_all / 1e6 / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -403,6 +407,7 @@ def run_ours(args, dist):
         ok = all(torch.equal(hd, d.cpu()) for hd, d in zip(hdists[:8], dists[:8]))
         e2e["matches_device_run"] = bool(ok)
         e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
+        e2e["calls"] = "asynchronous, one dtb_sync after the timed steps"
         # The same batch from separate pinned buffers per image (one copy per plane and direction).
         simgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
         smasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]

@@ -292,7 +292,10 @@ def geodesic_distance_transform(img, mask, gamma, v=DEFAULT_V, dist=None, *, rou
 
 def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=None, *, rounds=False, ctx=None,
                                       stream=None, asynchronous=False, timing=False):
-    """Ragged batch in one persistent launch over a shared tile queue (dtb_gdt_batch)."""
+    """Ragged batch in one persistent launch over a shared tile queue (dtb_gdt_batch).  With host tensors the
+    batch streams through the host-buffer pipeline.  ``asynchronous``: return after enqueueing (device tensors,
+    or all-host batches); ``ctx.sync(stream)`` waits and raises on a device error; the tensors must stay alive
+    and untouched until then."""
     n = len(imgs)
     imgs = [_as_tensor(t) for t in imgs]
     masks = [_as_tensor(t) for t in masks]

@@ -484,13 +484,14 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
 
   // Serialise with a previous asynchronous call on another stream (the scratch is shared).
   if (ctx->async_pending && ctx->last_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
+  if (ctx->pipe_pending && ctx->pipe_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
   ctx->async_pending = false;
 
   bool all_host = n > 0 && !(flags & DTB_FLAG_ROUNDS);
   for (int i = 0; i < n && all_host; ++i)
     all_host = jobs[i].mode == MODE_NS && imgs[i]->memory_kind == DTB_CPU && masks[i]->memory_kind == DTB_CPU &&
                dists[i]->memory_kind == DTB_CPU;
-  if (all_host) return run_host_pipeline(ctx, jobs, imgs, masks, dists, stream);
+  if (all_host) return run_host_pipeline(ctx, jobs, imgs, masks, dists, flags, stream);
 
   // ---- staging of inputs / outputs that are on the host or not aligned for TMA ----
   std::vector<Staged> staged;
@@ -700,6 +701,9 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
 DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (!ctx) return;
   if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
+  if (ctx->pipe_pending) cudaStreamSynchronize(ctx->pipe_stream);
+  if (ctx->dpipe) cudaFree(ctx->dpipe);
+  if (ctx->ev_pipe_done) cudaEventDestroy(ctx->ev_pipe_done);
   if (ctx->dscratch) cudaFree(ctx->dscratch);
   if (ctx->dround_counts) cudaFree(ctx->dround_counts);
   for (int i = 0; i < 2; ++i) {
@@ -757,6 +761,10 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream) {
   if (!ctx) return DTB_ERR_INVALID_ARG;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   DTB_CUDA(ctx, cudaStreamSynchronize(st));
+  if (ctx->pipe_pending) {
+    if (ctx->pipe_stream != st) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
+    return finish_pipeline(ctx);
+  }
   if (!ctx->async_pending) return DTB_OK;
   ctx->async_pending = false;
   const dtb_status s = read_device_status(ctx, ctx->last_hdr, &ctx->stats);

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "dtb.h"
@@ -44,6 +45,22 @@ __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restric
         if (b + k < it.row_bytes) v |= (uint32_t)s[b + k] << (8 * k);
       d[j] = v;
     }
+  }
+}
+
+// Folds the queue headers of a call's chunks into the context's accumulator: first error, counters summed.
+__global__ void pipe_fold(const uint8_t* __restrict__ scratch, const uint64_t* __restrict__ hdr_off, int nchunks,
+                          QueueHdr* acc) {
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < nchunks; ++k) {
+    const QueueHdr* h = reinterpret_cast<const QueueHdr*>(scratch + hdr_off[k]);
+    if (acc->error.v == 0 && h->error.v != 0) {
+      acc->error.v = h->error.v;
+      acc->err_info.v = h->err_info.v;
+    }
+    acc->progress.v += h->progress.v;
+    acc->phases.v += h->phases.v;
+    acc->activations.v += h->activations.v;
   }
 }
 
@@ -126,20 +143,30 @@ void place_plane(int a, int b, const std::vector<HostPlane>& hp, Take&& take, st
 }  // namespace
 
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
-                             const dtb_image* const* masks, const dtb_image* const* dists, cudaStream_t stream) {
+                             const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags,
+                             cudaStream_t stream) {
   const int n = (int)jobs.size();
   if (!ctx->s_in) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
   if (!ctx->s_lane) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_lane, cudaStreamNonBlocking));
+  if (!ctx->ev_pipe_done) DTB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_pipe_done, cudaEventDisableTiming));
+  if (!ctx->dpipe) {
+    DTB_CUDA(ctx, cudaMalloc(&ctx->dpipe, sizeof(QueueHdr)));
+    DTB_CUDA(ctx, cudaMemset(ctx->dpipe, 0, sizeof(QueueHdr)));
+  }
+  // A previous asynchronous call on another stream: finish it (its staging is about to be reused).
+  if (ctx->pipe_pending && ctx->pipe_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
 
-  // ---- chunks of about host_chunk_px pixels ----
+  // ---- chunks of about host_chunk_px pixels, the first ones smaller (1/8, 1/4, 1/2) so that the first maps
+  //      start their way back early ----
   std::vector<int> cut{0};
-  uint64_t acc = 0;
+  uint64_t acc = 0, target = std::max<uint64_t>(ctx->host_chunk_px / 8, 1);
   for (int i = 0; i < n; ++i) {
     acc += (uint64_t)jobs[i].width * jobs[i].height;
-    if (acc >= ctx->host_chunk_px && i + 1 < n) {
+    if (acc >= target && i + 1 < n) {
       cut.push_back(i + 1);
       acc = 0;
+      target = std::min<uint64_t>(2 * target, ctx->host_chunk_px);
     }
   }
   cut.push_back(n);
@@ -224,6 +251,8 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     o_items[k] = soff;
     soff = align_up(soff + sizeof(RepitchItem) * std::max<size_t>(items[k].size(), 1), 256);
   }
+  const size_t o_hoff = soff;  // chunk header offsets, for pipe_fold
+  soff = align_up(soff + 8ull * nchunks, 256);
   if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, soff)) != DTB_OK) return s;
   uint8_t* scratch = static_cast<uint8_t*>(ctx->dscratch);
   // Only the descriptor tables, tensor maps and repitch lists of each chunk go up (one pinned block, one copy
@@ -236,9 +265,16 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     h_items[k] = hbytes;
     hbytes += sizeof(RepitchItem) * items[k].size();
   }
+  const size_t h_hoff = hbytes;
+  hbytes += 8ull * nchunks;
   uint8_t* host = nullptr;
   cudaEvent_t ev_host = nullptr;
   if ((s = pinned_stage(ctx, hbytes, &host, &ev_host)) != DTB_OK) return s;
+  for (int k = 0; k < nchunks; ++k) {
+    const uint64_t off = o_chunk[k] + L[k].o_hdr;
+    std::memcpy(host + h_hoff + 8ull * k, &off, 8);
+  }
+  DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_hoff, host + h_hoff, 8ull * nchunks, cudaMemcpyHostToDevice, stream));
   for (int k = 0; k < nchunks; ++k) {
     std::vector<Job> cj(jobs.begin() + cut[k], jobs.begin() + cut[k + 1]);
     std::vector<uint8_t>& tab = ctx->hstage;
@@ -259,6 +295,7 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
 
   // ---- the pipeline ----
   DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ev_tables, 0));  // staging memory is free once earlier work is done
+  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pipe_done, 0));  // ... including the previous call's copies out
   for (int k = 0; k < nchunks; ++k) {
     for (const Copy& c : cin[k])
       if ((s = issue(ctx, c, stage, true, ctx->s_in)) != DTB_OK) return s;
@@ -288,32 +325,31 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     for (const Copy& c : cout[k])
       if ((s = issue(ctx, c, stage, false, ctx->s_out)) != DTB_OK) return s;
   }
-  cudaEvent_t e_done = event_at(ctx, 3 + 3 * (nchunks - 1));
-  if (!e_done) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
-  DTB_CUDA(ctx, cudaEventRecord(e_done, ctx->s_out));
-  DTB_CUDA(ctx, cudaStreamWaitEvent(stream, e_done, 0));
-  DTB_CUDA(ctx, cudaStreamSynchronize(stream));
-
-  // ---- status and counters of every chunk ----
-  dtb_stats acc_st{};
-  dtb_status first_err = DTB_OK;
-  for (int k = 0; k < nchunks; ++k) {
-    dtb_stats st{};
-    const dtb_status cs = read_device_status(ctx, reinterpret_cast<QueueHdr*>(scratch + o_chunk[k] + L[k].o_hdr), &st);
-    if (cs != DTB_OK && first_err == DTB_OK) first_err = cs;
-    acc_st.tiles += L[k].total;
-    acc_st.tile_visits += st.tile_visits;
-    acc_st.phases += st.phases;
-    acc_st.activations += st.activations;
-    if (!acc_st.device_error) {
-      acc_st.device_error = st.device_error;
-      acc_st.device_error_info = st.device_error_info;
-    }
-  }
-  acc_st.rounds = (uint64_t)nchunks;
-  ctx->stats = acc_st;
+  // Fold the chunks' status into the context's accumulator, then mark the call's end.
+  pipe_fold<<<1, 32, 0, ctx->s_out>>>(scratch, reinterpret_cast<const uint64_t*>(scratch + o_hoff), nchunks, ctx->dpipe);
+  DTB_CUDA(ctx, cudaGetLastError());
+  DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pipe_done, ctx->s_out));
+  DTB_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_pipe_done, 0));
+  ctx->pipe_tiles += total_all;
+  ctx->pipe_chunks += (uint64_t)nchunks;
+  ctx->pipe_pending = true;
+  ctx->pipe_stream = stream;
   ctx->async_pending = false;
-  return first_err;
+  if (flags & DTB_FLAG_ASYNC) return DTB_OK;  // dtb_sync(ctx, stream) waits and reports
+  DTB_CUDA(ctx, cudaStreamSynchronize(stream));
+  return finish_pipeline(ctx);
+}
+
+dtb_status finish_pipeline(dtb_context ctx) {
+  ctx->pipe_pending = false;
+  dtb_stats st{};
+  const dtb_status s = read_device_status(ctx, ctx->dpipe, &st);
+  st.tiles = ctx->pipe_tiles;
+  st.rounds = ctx->pipe_chunks;
+  ctx->stats = st;
+  ctx->pipe_tiles = ctx->pipe_chunks = 0;
+  DTB_CUDA(ctx, cudaMemset(ctx->dpipe, 0, sizeof(QueueHdr)));
+  return s;
 }
 
 }  // namespace dtb

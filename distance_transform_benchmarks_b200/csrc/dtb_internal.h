@@ -113,6 +113,13 @@ struct dtb_context_s {
   cudaEvent_t hpin_ev[2] = {nullptr, nullptr};
   bool hpin_used[2] = {false, false};
   int hpin_cur = 0;
+  // Host-buffer pipeline: status accumulated over the calls since the last dtb_sync (device, QueueHdr layout),
+  // completion of the last call, and its bookkeeping.
+  dtb::QueueHdr* dpipe = nullptr;
+  cudaEvent_t ev_pipe_done = nullptr;
+  bool pipe_pending = false;
+  cudaStream_t pipe_stream = nullptr;
+  uint64_t pipe_tiles = 0, pipe_chunks = 0;
   // Host-buffer pipeline: copy streams, a second compute lane, events, chunk size in pixels.
   cudaStream_t s_in = nullptr, s_out = nullptr, s_lane = nullptr;
   std::vector<cudaEvent_t> evpool;
@@ -159,8 +166,10 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_ima
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
 // All images, masks and distances in host memory (ns-mode): chunked pipeline of 1-D host-to-device copies,
 // repitch, tile runs and 1-D device-to-host copies on overlapping streams.
+// DTB_FLAG_ASYNC: returns after enqueueing; dtb_sync reports the status of all such calls since the last one.
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
-                             const dtb_image* const* masks, const dtb_image* const* dists, cudaStream_t stream);
+                             const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags,
+                             cudaStream_t stream);
 dtb_status grow(dtb_context ctx, void** p, size_t* size, size_t need);
 // Next pinned table-staging buffer of at least `need` bytes (waits until its previous copies are done);
 // *ev is to be recorded after the copies out of it.
@@ -182,5 +191,7 @@ Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns = D
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
 uint64_t tuning_key(int n, uint32_t total);
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);
+// Reads and clears the status accumulated by host-pipeline calls since the last read (the caller synchronised).
+dtb_status finish_pipeline(dtb_context ctx);
 
 }  // namespace dtb

@@ -53,7 +53,11 @@ typedef struct dtb_image {
 typedef struct dtb_context_s* dtb_context;
 
 /* Flags (bitwise or). */
-#define DTB_FLAG_ASYNC 0x1u       /* device images only: return after enqueueing; call dtb_sync() for the status */
+#define DTB_FLAG_ASYNC 0x1u       /* return after enqueueing; dtb_sync() waits and reports the status.  For images in
+                                     device memory, and for ns-mode batches whose images, masks and maps are all in
+                                     host memory (those must stay valid and untouched until dtb_sync returns; the
+                                     status covers every such call since the last dtb_sync).  Other host-memory
+                                     calls ignore the flag. */
 #define DTB_FLAG_ROUNDS 0x2u      /* plain per-image path: host-driven rounds over active tiles */
 #define DTB_FLAG_REF_NO_FMA 0x4u  /* ref-mode: round l_eucl*d and l_grad*|dI| separately instead of contracting */
 #define DTB_FLAG_TIMING 0x8u      /* record CUDA events around the tile kernel; dtb_stats.kernel_ms */

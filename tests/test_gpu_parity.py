@@ -243,6 +243,36 @@ def test_host_pipeline_arena_runs(chunk_kpx):
     c.close()
 
 
+def test_host_pipeline_asynchronous_calls():
+    """Back-to-back asynchronous host batches (the next call's copies wait for the previous call's) and one
+    dtb_sync for all of them; a stalled call among them is reported by that sync, and the context recovers."""
+    c = dtb.Context(0)
+    c.set_tuning(host_chunk_kpx=64)
+    batches = [wl.config3(seed=30 + k, n=9, smin=20, smax=200) for k in range(3)]
+    arenas = [dtb.host_batch_arena([i for i, _, _ in b], [m for _, m, _ in b]) for b in batches]
+    for b, (iv, mv, dv) in zip(batches, arenas):
+        dtb.geodesic_distance_transform_batch(iv, mv, [g for _, _, g in b], dists=dv, ctx=c, asynchronous=True)
+    c.sync()
+    for b, (_, _, dv) in zip(batches, arenas):
+        for k, (img, mask, g) in enumerate(b):
+            assert_images_eq(dv[k], orc.ggdt_ns(img, mask, g), "async batch image %d" % k)
+    st = c.stats()
+    assert st["tiles"] == sum(sum(((i.shape[0] + 31) // 32) * ((i.shape[1] + 31) // 32) for i, _, _ in b) for b in batches)
+    # A stalled call in the middle: the sync raises; the next synchronous call is correct.
+    iv, mv, dv = arenas[0]
+    gam = [g for _, _, g in batches[0]]
+    dtb.geodesic_distance_transform_batch(iv, mv, gam, dists=dv, ctx=c, asynchronous=True)
+    c.inject_queue_stall(100)
+    dtb.geodesic_distance_transform_batch(iv, mv, gam, dists=dv, ctx=c, asynchronous=True)
+    with pytest.raises(dtb.DtbError) as e:
+        c.sync()
+    assert e.value.status == 4
+    dtb.geodesic_distance_transform_batch(iv, mv, gam, dists=dv, ctx=c)
+    for k, (img, mask, g) in enumerate(batches[0]):
+        assert_images_eq(dv[k], orc.ggdt_ns(img, mask, g), "after stall, image %d" % k)
+    c.close()
+
+
 def test_batch_host_buffers(ctx):
     batch = wl.config3(seed=12, n=6, smin=40, smax=200)
     dists = dtb.geodesic_distance_transform_batch([torch.from_numpy(i) for i, _, _ in batch],
