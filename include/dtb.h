@@ -193,7 +193,7 @@ DTB_API void dtb_serve_destroy(dtb_server s);
  * For callers that must not allocate device memory behind their own allocator: a host that owns all device
  * memory through its own pool or budget, or a loop that cannot afford the device-wide synchronisation of
  * cudaMalloc / cudaFree.  No context: the scratch is a fixed array in the library's device memory (about
- * 322 KB on every GPU that loads the library, held until exit), so the image may have at most 16384 tiles of
+ * 324 KB on every GPU that loads the library, held until exit), so the image may have at most 16384 tiles of
  * 32 x 32 pixels (e.g. 4096 x 4096); larger images return DTB_ERR_CAPACITY.  img, mask and dist must be device
  * memory, img and mask with 16-byte aligned buffer and pitch, dist with 4-byte alignment (no staging copies);
  * otherwise DTB_ERR_INVALID_ARG.  Synchronous: returns after the map is written.  The first call on a device
