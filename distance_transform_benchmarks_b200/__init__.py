@@ -20,7 +20,7 @@ from ._native import (DTB_CPU, DTB_FLAG_ASYNC, DTB_FLAG_REF_NO_FMA, DTB_FLAG_ROU
                       DtbServeRequest, DtbServeStats, DtbStats, DtbTuning, lib)
 
 __all__ = [
-    "Context", "DtbError", "default_context", "generalised_distance_transform",
+    "Context", "DtbError", "default_context", "generalised_distance_transform", "imread", "imsave",
     "generalised_distance_transform_blocks", "generalised_distance_transform_task", "geodesic_distance_transform",
     "geodesic_distance_transform_batch", "host_to_device", "device_to_host", "image_view", "DEFAULT_V", "BatchPlan",
     "pitched_empty", "pitched_from", "Server",
@@ -317,6 +317,35 @@ def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=No
     ctx.check(lib().dtb_gdt_batch(ctx.handle, n, vi, vm, vd, g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(v),
                                   flags, ctypes.c_void_p(_stream_ptr(stream))))
     return dists
+
+
+def imread(path, channels=1):
+    """dt::imread (reference dt/src/imread.cpp): an 8-bit PNG / PGM / PPM file as a uint8 array, [H, W] for
+    channels=1 (the file must be gray), [H, W, 3] for channels=3 (rgb or palette)."""
+    im = DtbImage()
+    st = lib().dtb_image_read(str(path).encode(), int(channels), ctypes.byref(im))
+    if st != 0:
+        raise DtbError(st, "cannot read %s as a %d-channel 8-bit image" % (path, channels))
+    try:
+        buf = (ctypes.c_uint8 * (im.pitch * im.height)).from_address(im.buffer)
+        a = np.frombuffer(buf, dtype=np.uint8).reshape(im.height, im.pitch)[:, :im.width * channels]
+        out = a.reshape(im.height, im.width, channels).copy() if channels == 3 else a.copy()
+    finally:
+        lib().dtb_image_free(ctypes.byref(im))
+    return out
+
+
+def imsave(path, img):
+    """dt::imsave (reference dt/src/imsave.cpp): a uint8 [H, W] or [H, W, 3] array (or tensor) to .png, .pgm
+    (gray) or .ppm (rgb8)."""
+    t = _as_tensor(img)
+    if t.is_cuda:
+        t = t.cpu()
+    t = t.contiguous()
+    view = image_view(t, 3 if t.dim() == 3 else 1)
+    st = lib().dtb_image_write(str(path).encode(), ctypes.byref(view))
+    if st != 0:
+        raise DtbError(st, "cannot write %s" % path)
 
 
 def host_to_device(t, stream=None):

@@ -19,7 +19,7 @@ DTB_FLAG_TIMING = 0x8
 
 STATUS_NAMES = {
     0: "DTB_OK", 1: "DTB_ERR_INVALID_ARG", 2: "DTB_ERR_CUDA", 3: "DTB_ERR_OUT_OF_MEMORY", 4: "DTB_ERR_TIMEOUT",
-    5: "DTB_ERR_DEVICE", 6: "DTB_ERR_NO_DEVICE", 7: "DTB_ERR_CAPACITY",
+    5: "DTB_ERR_DEVICE", 6: "DTB_ERR_NO_DEVICE", 7: "DTB_ERR_CAPACITY", 8: "DTB_ERR_IO",
 }
 
 # Every symbol include/dtb.h declares (checked by the CPU test suite).
@@ -29,7 +29,7 @@ DTB_SYMBOLS = [
     "dtb_device_to_host", "dtb_context_set_tuning", "dtb_context_get_tuning", "dtb_plan_create", "dtb_plan_run",
     "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy", "dtb_serve_create", "dtb_serve_submit", "dtb_serve_poll",
     "dtb_serve_release", "dtb_serve_get_stats", "dtb_serve_destroy", "dtb_gdt_ref_blocks", "dtb_image_alloc",
-    "dtb_image_free", "dtb_debug_inject_queue_stall",
+    "dtb_image_free", "dtb_debug_inject_queue_stall", "dtb_image_read", "dtb_image_write",
 ]
 
 DTB_REQ_IMAGE = 0
@@ -129,6 +129,10 @@ def lib():
         L.dtb_image_alloc.argtypes = [I32, I32, I32, I32, ctypes.POINTER(DtbImage)]
         L.dtb_debug_inject_queue_stall.restype = I32
         L.dtb_debug_inject_queue_stall.argtypes = [P, U32]
+        L.dtb_image_read.restype = I32
+        L.dtb_image_read.argtypes = [ctypes.c_char_p, I32, ctypes.POINTER(DtbImage)]
+        L.dtb_image_write.restype = I32
+        L.dtb_image_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(DtbImage)]
         L.dtb_image_free.restype = I32
         L.dtb_image_free.argtypes = [ctypes.POINTER(DtbImage)]
         L.dtb_gdt_batch.restype = I32

@@ -64,13 +64,13 @@ def _deps(*names):
 
 def build_dtb(force=False, verbose=False, ptxas_verbose=False):
     out = os.path.join(HERE, "libdtb.so")
-    srcs = ["dtb_api.cu", "dtb_plan.cu", "dtb_host_pipeline.cu", "dtb_serve.cu", "dtb_noalloc.cu"]
+    srcs = ["dtb_api.cu", "dtb_plan.cu", "dtb_host_pipeline.cu", "dtb_serve.cu", "dtb_noalloc.cu", "dtb_io.cpp"]
     srcs = [s for s in srcs if os.path.exists(os.path.join(CSRC, s))]
     if force or _stale(out, _deps(*srcs)):
         cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC, "-shared", "-o", out]
         if ptxas_verbose:
             cmd += ["-Xptxas", "-v"]
-        cmd += [os.path.join(CSRC, s) for s in srcs]
+        cmd += [os.path.join(CSRC, s) for s in srcs] + ["-lz"]  # zlib: PNG files (dtb_io.cpp)
         r = _run(cmd, verbose)
         if ptxas_verbose:
             sys.stdout.write(r.stderr)

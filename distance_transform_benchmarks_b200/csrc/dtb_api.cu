@@ -638,6 +638,7 @@ DTB_API const char* dtb_status_string(dtb_status s) {
     case DTB_ERR_DEVICE: return "device-side error";
     case DTB_ERR_NO_DEVICE: return "no usable device";
     case DTB_ERR_CAPACITY: return "capacity exceeded";
+    case DTB_ERR_IO: return "image file could not be read or written";
   }
   return "unknown status";
 }

@@ -10,6 +10,7 @@
 
 #include <cassert>
 #include <cstdint>
+#include <type_traits>
 #include <utility>
 
 #include "dtb.h"
@@ -101,7 +102,8 @@ namespace dt
   public:
     image2d_view() noexcept = default;
     image2d_view(T* buffer, int width, int height, int pitch, e_memory_kind memory_kind = e_memory_kind::CPU) noexcept
-      : image2d_view<void>(reinterpret_cast<std::uint8_t*>(buffer), width, height, pitch, sizeof(T), memory_kind)
+      : image2d_view<void>(reinterpret_cast<std::uint8_t*>(const_cast<std::remove_const_t<T>*>(buffer)), width, height,
+                           pitch, sizeof(T), memory_kind)
     {
     }
 

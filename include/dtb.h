@@ -31,7 +31,8 @@ typedef enum dtb_status {
   DTB_ERR_TIMEOUT = 4,       /* a bounded device wait gave up (no progress); the result is invalid */
   DTB_ERR_DEVICE = 5,        /* the kernel reported an internal error (phase limit, ring full) */
   DTB_ERR_NO_DEVICE = 6,     /* no usable sm_100 device */
-  DTB_ERR_CAPACITY = 7       /* a fixed-size limit was exceeded */
+  DTB_ERR_CAPACITY = 7,      /* a fixed-size limit was exceeded */
+  DTB_ERR_IO = 8             /* an image file could not be read or written (reference: std::runtime_error, imread.cpp:15-16) */
 } dtb_status;
 
 /* Memory kinds, reference dt::e_memory_kind (dt/include/dt/image2d_view.hpp:9-13). */
@@ -216,6 +217,15 @@ DTB_API dtb_status dtb_debug_inject_queue_stall(dtb_context ctx, uint32_t timeou
  * dtb_image_free releases it (NULL buffer: no-op) and clears out->buffer. */
 DTB_API dtb_status dtb_image_alloc(int32_t width, int32_t height, int32_t elem_size, int32_t memory_kind, dtb_image* out);
 DTB_API dtb_status dtb_image_free(dtb_image* img);
+
+/* Image files, reference dt::imread / dt::imsave (dt/include/dt/imread.hpp:7-8, imsave.hpp:13-43; the reference
+ * reads any stb_image format and writes PNG).  Formats: PNG (read: gray, gray + alpha, rgb, rgba, palette at 8 bits
+ * per sample, gray and palette also at 1 / 2 / 4, not interlaced; write: 8-bit gray or rgb) and binary PGM / PPM, chosen by the file name (.png, .pgm, .ppm) on write
+ * and by the contents on read.  dtb_image_read: `channels` 1 (gray) or 3 (rgb8) must match the file's
+ * components, as the reference requires one component for imread<uint8_t>; the pixels go into new host memory
+ * (free with dtb_image_free).  dtb_image_write: a host image of elem_size 1 or 3. */
+DTB_API dtb_status dtb_image_read(const char* path, int32_t channels, dtb_image* out);
+DTB_API dtb_status dtb_image_write(const char* path, const dtb_image* img);
 
 /* Host <-> device copies of a pitched image, reference dt::host_to_device / dt::device_to_host
  * (dt/include/dt/transfert.hpp:13-15, dt/src/transfert.cpp:10-28).  Synchronous when stream is NULL. */

@@ -25,7 +25,7 @@ def build(force=False):
     return LIB_PATH
 
 
-REF_TESTS = ("image_view", "image2d", "c4", "rgb8", "transfert", "distance_transform")
+REF_TESTS = ("image_view", "image2d", "c4", "rgb8", "io", "transfert", "distance_transform")
 
 
 def build_ref(ref_root, force=False):

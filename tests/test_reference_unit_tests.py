@@ -13,19 +13,19 @@ import pytest
 from oracle import oracle as orc
 
 
-def _run(name):
+def _run(name, cwd=None):
     exe = orc.ref_test_binary(name)
     if exe is None:
         pytest.skip("oracle/_ref/test_%s not built (reference source tree absent at build time)" % name)
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600, cwd=cwd)
     assert r.returncode == 0, r.stdout + r.stderr
     assert " 0 failed" in r.stdout, r.stdout
     return r.stdout
 
 
-@pytest.mark.parametrize("name", ["image_view", "image2d", "c4", "rgb8"])
-def test_reference_host_unit_tests(name):
-    _run(name)
+@pytest.mark.parametrize("name", ["image_view", "image2d", "c4", "rgb8", "io"])
+def test_reference_host_unit_tests(name, tmp_path):
+    _run(name, cwd=str(tmp_path))  # io writes its file into the working directory
 
 
 @pytest.mark.gpu
