@@ -408,6 +408,7 @@ def run_ours(args, dist):
         e2e["matches_device_run"] = bool(ok)
         e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
         e2e["calls"] = "asynchronous, one dtb_sync after the timed steps"
+    if e2e is not None and dist.world == 1:
         # The same batch from separate pinned buffers per image (one copy per plane and direction).
         simgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
         smasks = [torch.from_numpy(m).pin_memory() for _, m, _ in batch]
@@ -435,9 +436,11 @@ def run_ours(args, dist):
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batch, CPU_SAMPLE_SECONDS)
-    ref_mode = None if args.no_ref_mode else run_ref_mode(args, ctx, stream)
+    # The reference-shape and serving legs run in single-GPU runs only (with N ranks every rank would repeat
+    # them on its own GPU; the job's line reports the batch and e2e legs, reduced over ranks).
+    ref_mode = None if (args.no_ref_mode or dist.world > 1) else run_ref_mode(args, ctx, stream)
     serve = None
-    if not args.no_serve:
+    if not args.no_serve and dist.world == 1:
         himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
         serve = run_serve(args, dev)
 
