@@ -471,6 +471,9 @@ def run_ours(args, dist):
 def main():
     args = parse()
     dist = Dist()
+    if dist.world > 1 and "OMP_NUM_THREADS" not in os.environ:
+        # The ranks share the host: split its cores for the input generators.
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // dist.world))
     if args.impl == "reference":
         run_reference(args, dist)  # rank 0 only; the other ranks exit without work
         return
