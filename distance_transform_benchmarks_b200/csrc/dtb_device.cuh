@@ -154,14 +154,17 @@ __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
 }
 
 // ------------------------------------------------------------------------------------------------------
-// Queue: a ticket ring of tile ids with a pending counter for termination.
-//   push: pending grows first, then a tail range is reserved, then each item goes into its slot (the slot
-//         must be free: CAS from 0).
-//   pop:  a head ticket, then the popper waits on its own slot only (no shared hot line is polled), until
-//         an item or the termination sentinel arrives.  Termination: the visit whose completion brings
-//         pending to 0 sets `done` and writes the sentinel into every slot that has a waiting popper.
+// Queue: one or NBUCKET ticket rings of tile ids (buckets ordered by distance) with one pending counter for
+// termination.
+//   push: pending grows first, then a position of the item's bucket is reserved, then the item goes into its
+//         slot (the slot must be free: CAS from 0; a slot given back by a waiter is skipped).
+//   pop:  a head ticket in the lowest bucket holding work (or in the base bucket when there is none), then the
+//         popper waits on its own slot only (no shared hot line is polled) until an item or the termination
+//         sentinel arrives; in the bucketed queue a waiter whose item is not reserved gives the ticket back
+//         when another bucket holds work.  Termination: the visit whose completion brings pending to 0 sets
+//         `done` and writes the sentinel into every slot that has a waiting popper.
 // Items are interchangeable, so a popper that takes an item meant for another ticket of the same slot is
-// harmless: every item is taken exactly once (atomicExch) and no slot is written twice (CAS from 0).  The
+// harmless: every item is taken exactly once (atomicExch) and no slot is written twice (CAS from 0).  Each
 // ring holds at least 2 * (tiles + workers) slots, more than items and waiting poppers together.
 // All waits are bounded by a no-global-progress watchdog and end with an error code, never a hang.
 // ------------------------------------------------------------------------------------------------------
