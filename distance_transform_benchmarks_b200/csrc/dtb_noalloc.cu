@@ -6,8 +6,8 @@
 // cudaMalloc / cudaFree imply.  The regular entry points keep their scratch in a dtb_context, which allocates;
 // this one keeps it in a fixed file-scope device array instead, so a call allocates nothing.
 //
-// The scratch (queue header, one state word per tile, one FIFO ticket ring (no priority buckets), the image descriptor and its two TMA
-// tensor maps) lives in g_noalloc_scratch below: NOALLOC_BYTES (about 324 KB) on every GPU that loads the
+// The scratch (queue header, one state word per tile, one FIFO ticket ring -- no priority buckets -- and the
+// image descriptor with its two TMA tensor maps) lives in g_noalloc_scratch below: NOALLOC_BYTES (about 324 KB) on every GPU that loads the
 // library, held until the process exits.  It bounds the image to NOALLOC_MAX_TILES tiles of 32 x 32 pixels.
 // All calls share the array and find the previous call's contents there; every call clears the queue header
 // and the ring before use and rewrites the rest.  Two calls that overlap on the GPU (different host threads or
