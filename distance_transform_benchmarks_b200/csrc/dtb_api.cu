@@ -238,7 +238,9 @@ dtb_status check_triplet(dtb_context ctx, const dtb_image* img, const dtb_image*
 dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* total) {
   uint64_t t = 0;
   for (const Job& j : jobs) t += (uint64_t)j.tiles_x() * j.tiles_y();
-  if (t >= (1ull << 31) || jobs.size() >= (1u << 23))
+  // 2^28 tiles (275 Gpx) is far beyond device memory; the limit keeps the ring capacity (a power of two >=
+  // 2 * (tiles + workers)) and the 31-bit tile ids of the queue items in range.
+  if (t >= (1ull << 28) || jobs.size() >= (1u << 23))
     return fail(ctx, DTB_ERR_CAPACITY, "too many tiles (%llu) or images (%zu)", (unsigned long long)t, jobs.size());
   *total = (uint32_t)t;
   return DTB_OK;
@@ -254,7 +256,7 @@ ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, u
   ScratchLayout L;
   L.n = n;
   L.total = total;
-  L.cap = next_pow2(2u * (total + workers + 64u));
+  L.cap = next_pow2((uint32_t)std::min<uint64_t>(2ull * ((uint64_t)total + workers + 64u), 1ull << 31));
   L.nb = buckets > 1 ? NBUCKET : 1u;
   size_t off = 0;
   L.o_hdr = off;    off = align_up(off + sizeof(QueueHdr), 256);
