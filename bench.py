@@ -151,8 +151,31 @@ def cpu_baseline(batch, seconds):
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
-    return {"value": px / dt / 1e6, "unit": UNIT, "cores": orc.max_threads(), "kind": "port",
-            "sample": "first %d images of the batch (%.1f Mpx), %.1f s" % (n, px / 1e6, dt)}
+    out = {"value": px / dt / 1e6, "unit": UNIT, "cores": orc.max_threads(), "kind": "port",
+           "sample": "first %d images of the batch (%.1f Mpx), %.1f s" % (n, px / 1e6, dt)}
+
+    def rate(fn, seconds):
+        px, t0 = 0, time.perf_counter()
+        for img, mask, g in batch:
+            fn(img, mask, g)
+            px += img.shape[0] * img.shape[1]
+            if time.perf_counter() - t0 > seconds:
+                break
+        return px / (time.perf_counter() - t0) / 1e6
+
+    # For information (same images, a few seconds each): one host thread, the FP64 Dijkstra on the same graph
+    # (one thread), and the reference weight (C8, lambda 0.5; the raster restatement is single-threaded).
+    out["single_thread_mpx_s"] = rate(lambda i, m, g: orc.ggdt_ns(i, m, g, nthreads=1), 3.0)
+    out["dijkstra_f64_mpx_s"] = rate(lambda i, m, g: orc.dijkstra_ns_f64(i, m, g), 3.0)
+    gray = [(i, m, g) for i, m, g in batch if i.ndim == 2]
+    px, t0 = 0, time.perf_counter()
+    for img, mask, _ in gray:
+        orc.ggdt_ref(img, mask, 0.5)
+        px += img.size
+        if time.perf_counter() - t0 > 3.0:
+            break
+    out["ref_mode_lambda05_single_thread_mpx_s"] = px / (time.perf_counter() - t0) / 1e6
+    return out
 
 
 SERVE_POOL = 48                 # distinct synthetic images behind the new-image requests
