@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--serve-rate", type=float, default=500.0, help="Poisson arrival rate (requests / s)")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-ref-mode", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the single-image C0 / C1 / C2 leg")
     p.add_argument("--ref-mpx", type=float, default=REF_STEP_MPX, help="reference arm: pixels per step (millions)")
     return p.parse_args()
 
@@ -220,6 +221,34 @@ def run_ref_mode(args, ctx, stream):
             "reference_published_mpx_s": REF_PUBLISHED,
             "note": "whole call timed on the stream (allocation + setup + transform), inputs resident on the device; "
                     "task = persistent tile queue (the raster variant returns the same map through the same path)"}
+
+
+def run_configs(ctx, stream):
+    """The single-image configurations, inputs resident on the device, one call each (3 timed): C0 (512^2 gray
+    blobs), C1 (4096^2 gray maze: the worst case for raster passes, paths wind through the whole image) and C2
+    (8192^2 rgb8 Voronoi), with the tile visits and sweep phases behind each figure."""
+    import distance_transform_benchmarks_b200 as dtb
+    from distance_transform_benchmarks_b200 import workloads as wl
+    out = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, gen in (("C0", wl.config0), ("C1", wl.config1), ("C2", wl.config2)):
+        img, mask, gamma = gen()
+        ti, tm = dtb.pitched_from(img), dtb.pitched_from(mask)
+        d = dtb.pitched_empty(img.shape[0], img.shape[1], 1, torch.float32)
+        dtb.geodesic_distance_transform(ti, tm, gamma, dist=d, ctx=ctx, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            dtb.geodesic_distance_transform(ti, tm, gamma, dist=d, ctx=ctx, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        st = ctx.stats()
+        out[name] = {"shape": list(img.shape), "ms": ms, "mpx_s": img.shape[0] * img.shape[1] / 1e3 / ms,
+                     "visits_per_tile": st["tile_visits"] / max(1, st["tiles"]),
+                     "phases_per_visit": st["phases"] / max(1, st["tile_visits"]),
+                     "activations_per_tile": st["activations"] / max(1, st["tiles"])}
+    return out
 
 
 def run_serve(args, dev):
@@ -462,6 +491,7 @@ def run_ours(args, dist):
     # The reference-shape and serving legs run in single-GPU runs only (with N ranks every rank would repeat
     # them on its own GPU; the job's line reports the batch and e2e legs, reduced over ranks).
     ref_mode = None if (args.no_ref_mode or dist.world > 1) else run_ref_mode(args, ctx, stream)
+    configs = None if (args.no_configs or dist.world > 1) else run_configs(ctx, stream)
     serve = None
     if not args.no_serve and dist.world == 1:
         himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
@@ -485,7 +515,7 @@ def run_ours(args, dist):
                                "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},
                 "gpu_launches": 3 * args.steps,
                 "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serve": serve,
-                "ref_mode": ref_mode}
+                "ref_mode": ref_mode, "configs": configs}
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()
