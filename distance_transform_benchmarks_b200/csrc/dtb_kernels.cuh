@@ -38,12 +38,26 @@ struct QueueSched {
   // a re-run requested meanwhile re-queues it at the smallest value its activators left in keys[].  `pending`
   // moves by (pushes - 1) in one atomic performed before any push is visible; the visit that brings it to 0
   // ends the queue.
+  // The own-tile update comes first and, when it sets VISITED, is fenced before the activations: a woken
+  // neighbour takes this tile's distances as halo only if it sees VISITED, and otherwise reads v in their
+  // place.  Seeing the activation without the bit would consume the wake-up without the new distances.
   __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item,
                                            float key = 0.0f, float inv_width = 0.0f) const {
     const int lane = threadIdx.x & 31;
     bool push = false;
     uint32_t item = 0;
     float pkey = key;
+    if (lane == 31) {
+      const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
+      push = (old & ST_PENDING) != 0u;
+      item = tile;
+      if (push && q.keys) {
+        const uint32_t kb = ld_volatile(&q.keys[tile]);
+        pkey = kb == KEY_NONE ? 0.0f : __uint_as_float(kb);
+      }
+      if (xor_bits & ST_VISITED) __threadfence();
+    }
+    __syncwarp();
     if (want) {
       if (want_item >= q.total_tiles) {
         set_error(q, DERR_BAD_TILE, want_item);
@@ -55,15 +69,6 @@ struct QueueSched {
         const uint32_t old = atomicOr(&states[want_item], ST_PENDING);
         push = !(old & (ST_PENDING | ST_RUNNING));
         item = want_item;
-      }
-    }
-    if (lane == 31) {
-      const uint32_t old = atomicXor(&states[tile], xor_bits | ST_RUNNING);
-      push = (old & ST_PENDING) != 0u;
-      item = tile;
-      if (push && q.keys) {
-        const uint32_t kb = ld_volatile(&q.keys[tile]);
-        pkey = kb == KEY_NONE ? 0.0f : __uint_as_float(kb);
       }
     }
     const uint32_t m = __ballot_sync(~0u, push);
@@ -131,6 +136,10 @@ __device__ __forceinline__ float f_inf() { return __int_as_float(0x7f800000); }
 __device__ __forceinline__ float* dist_row(const ImgDesc& dd, int y) {
   return reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(dd.dist) + (int64_t)y * dd.dist_pitch);
 }
+
+// Distance read of a pixel that another warp (on any SM) may have written during this launch: L2 only, so no
+// line an SM cached earlier can be returned.
+__device__ __forceinline__ float ld_dist(const ImgDesc& dd, int y, int x) { return __ldcg(dist_row(dd, y) + x); }
 
 // Waits for the TMA transactions of this warp's slot.  Bounded: on timeout the error word is set and the
 // wait goes on (bounded again) so that no copy is left in flight when the warp leaves.
@@ -224,19 +233,19 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Halo: column layout for top/bottom (lane = x), row layout for left/right (lane = y).
   float top = INF, bot = INF, lft = INF, rgt = INF;
   if (lane < vw) {
-    if (nexist & 4u) top = (nvis & 4u) ? dist_row(dd, y0 - 1)[x0 + lane] : v;
-    if (nexist & 8u) bot = (nvis & 8u) ? dist_row(dd, y0 + TILE)[x0 + lane] : v;
+    if (nexist & 4u) top = (nvis & 4u) ? ld_dist(dd, y0 - 1, x0 + lane) : v;
+    if (nexist & 8u) bot = (nvis & 8u) ? ld_dist(dd, y0 + TILE, x0 + lane) : v;
   }
   if (lane < vh) {
-    if (nexist & 1u) lft = (nvis & 1u) ? dist_row(dd, y0 + lane)[x0 - 1] : v;
-    if (nexist & 2u) rgt = (nvis & 2u) ? dist_row(dd, y0 + lane)[x0 + TILE] : v;
+    if (nexist & 1u) lft = (nvis & 1u) ? ld_dist(dd, y0 + lane, x0 - 1) : v;
+    if (nexist & 2u) rgt = (nvis & 2u) ? ld_dist(dd, y0 + lane, x0 + TILE) : v;
   }
 
   // Tile distances in column layout.
   float d[TILE];
   if (!first) {
 #pragma unroll
-    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? dist_row(dd, y0 + y)[x0 + lane] : INF;
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
   }
 
   if (!tma_wait(sm, parity, sch.q, tile)) return;
@@ -518,7 +527,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   auto halo_val = [&](int k, int gx, int gy) -> float {  // neighbour k's pixel (gx, gy)
     if (!((nexist >> k) & 1u)) return INF;
     if (gx >= dd.width || gy >= dd.height) return INF;
-    return ((nvis >> k) & 1u) ? dist_row(dd, gy)[gx] : v;
+    return ((nvis >> k) & 1u) ? ld_dist(dd, gy, gx) : v;
   };
   ht[lane + 1] = (lane < vw) ? halo_val(2, x0 + lane, y0 - 1) : INF;
   hb[lane + 1] = (lane < vw) ? halo_val(3, x0 + lane, y0 + TILE) : INF;
@@ -536,7 +545,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   float d[TILE];
   if (!first) {
 #pragma unroll
-    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? dist_row(dd, y0 + y)[x0 + lane] : INF;
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
   }
 
   if (!tma_wait(sm, parity, sch.q, tile)) return;
