@@ -484,9 +484,9 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   const int n = (int)jobs_in.size();
   std::vector<Job> jobs = jobs_in;
 
-  // Serialise with a previous asynchronous call on another stream (the scratch is shared).
+  // Serialise with a previous asynchronous call on another stream (the scratch is shared; host-buffer pipeline
+  // calls have their own).
   if (ctx->async_pending && ctx->last_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->last_stream));
-  if (ctx->pipe_pending && ctx->pipe_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
   ctx->async_pending = false;
 
   bool all_host = n > 0 && !(flags & DTB_FLAG_ROUNDS);
@@ -704,9 +704,15 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
 DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (!ctx) return;
   if (ctx->async_pending) cudaStreamSynchronize(ctx->last_stream);
-  if (ctx->pipe_pending) cudaStreamSynchronize(ctx->pipe_stream);
+  if (ctx->pipe_pending) cudaEventSynchronize(ctx->ev_pipe_done);
   if (ctx->dpipe) cudaFree(ctx->dpipe);
   if (ctx->ev_pipe_done) cudaEventDestroy(ctx->ev_pipe_done);
+  if (ctx->ev_pipe_start) cudaEventDestroy(ctx->ev_pipe_start);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->pstage[i]) cudaFree(ctx->pstage[i]);
+    if (ctx->pscratch[i]) cudaFree(ctx->pscratch[i]);
+    if (ctx->ev_pset_free[i]) cudaEventDestroy(ctx->ev_pset_free[i]);
+  }
   if (ctx->dscratch) cudaFree(ctx->dscratch);
   if (ctx->dround_counts) cudaFree(ctx->dround_counts);
   for (int i = 0; i < 2; ++i) {
@@ -721,6 +727,7 @@ DTB_API void dtb_context_destroy(dtb_context ctx) {
   if (ctx->s_in) cudaStreamDestroy(ctx->s_in);
   if (ctx->s_out) cudaStreamDestroy(ctx->s_out);
   if (ctx->s_lane) cudaStreamDestroy(ctx->s_lane);
+  if (ctx->s_lane0) cudaStreamDestroy(ctx->s_lane0);
   delete ctx;
 }
 
@@ -765,7 +772,7 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   DTB_CUDA(ctx, cudaStreamSynchronize(st));
   if (ctx->pipe_pending) {
-    if (ctx->pipe_stream != st) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
+    DTB_CUDA(ctx, cudaEventSynchronize(ctx->ev_pipe_done));  // the last call's end (copies out run in call order)
     return finish_pipeline(ctx);
   }
   if (!ctx->async_pending) return DTB_OK;

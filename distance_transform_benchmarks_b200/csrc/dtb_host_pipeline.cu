@@ -7,9 +7,11 @@
 // it (rows or bases not on 16 bytes), and writes distances packed in the mirrored layout so that each run
 // returns as one 1-D copy.  The batch is cut into chunks of about host_chunk_px pixels; the copies in (stream
 // s_in), the tile runs and the copies out (stream s_out) of successive chunks overlap.  The tile runs alternate
-// between two compute lanes (the caller's stream and s_lane), each launched on half of the co-resident CTAs:
-// a run's tail, where only the last tiles of its largest images are still active, then overlaps the next
-// chunk's run instead of idling the GPU (one lane ran each chunk at about a third of the batch rate).
+// between two compute lanes (s_lane0, s_lane), each launched on half of the co-resident CTAs: a run's tail,
+// where only the last tiles of its largest images are still active, then overlaps the next chunk's run instead
+// of idling the GPU (one lane ran each chunk at about a third of the batch rate).  Successive calls use
+// alternate sets of device staging and scratch, so a call's copies in run while the previous call's copies
+// out finish (the two directions of the link overlap across calls as well as within one).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -149,13 +151,17 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   if (!ctx->s_in) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));
   if (!ctx->s_lane) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_lane, cudaStreamNonBlocking));
+  if (!ctx->s_lane0) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_lane0, cudaStreamNonBlocking));
   if (!ctx->ev_pipe_done) DTB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_pipe_done, cudaEventDisableTiming));
+  if (!ctx->ev_pipe_start) DTB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_pipe_start, cudaEventDisableTiming));
+  for (int i = 0; i < 2; ++i)
+    if (!ctx->ev_pset_free[i]) DTB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_pset_free[i], cudaEventDisableTiming));
   if (!ctx->dpipe) {
     DTB_CUDA(ctx, cudaMalloc(&ctx->dpipe, sizeof(QueueHdr)));
     DTB_CUDA(ctx, cudaMemset(ctx->dpipe, 0, sizeof(QueueHdr)));
   }
-  // A previous asynchronous call on another stream: finish it (its staging is about to be reused).
-  if (ctx->pipe_pending && ctx->pipe_stream != stream) DTB_CUDA(ctx, cudaStreamSynchronize(ctx->pipe_stream));
+  const int set = ctx->pset_cur;
+  ctx->pset_cur ^= 1;
 
   // ---- chunks of about host_chunk_px pixels, the first ones smaller (1/8, 1/4, 1/2) so that the first maps
   //      start their way back early ----
@@ -202,9 +208,9 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     o_it[i] = (rb % 16 || o_ip[i] % 16) ? take(align_up(rb, 128) * h) : o_ip[i];
     o_mt[i] = ((size_t)j.width % 16 || o_mp[i] % 16) ? take(align_up((size_t)j.width, 128) * h) : o_mp[i];
   }
-  dtb_status s = grow(ctx, &ctx->dstage, &ctx->dstage_size, off);
+  dtb_status s = grow(ctx, &ctx->pstage[set], &ctx->pstage_size[set], off);
   if (s != DTB_OK) return s;
-  uint8_t* stage = static_cast<uint8_t*>(ctx->dstage);
+  uint8_t* stage = static_cast<uint8_t*>(ctx->pstage[set]);
   for (int i = 0; i < n; ++i) {
     const int64_t rb = (int64_t)jobs[i].width * jobs[i].channels;
     jobs[i].img = stage + o_it[i];
@@ -253,8 +259,8 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   }
   const size_t o_hoff = soff;  // chunk header offsets, for pipe_fold
   soff = align_up(soff + 8ull * nchunks, 256);
-  if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, soff)) != DTB_OK) return s;
-  uint8_t* scratch = static_cast<uint8_t*>(ctx->dscratch);
+  if ((s = grow(ctx, &ctx->pscratch[set], &ctx->pscratch_size[set], soff)) != DTB_OK) return s;
+  uint8_t* scratch = static_cast<uint8_t*>(ctx->pscratch[set]);
   // Only the descriptor tables, tensor maps and repitch lists of each chunk go up (one pinned block, one copy
   // per part); queue headers, rings and tile states are reset on the device by each chunk's run.
   size_t hbytes = 0;
@@ -270,11 +276,16 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   uint8_t* host = nullptr;
   cudaEvent_t ev_host = nullptr;
   if ((s = pinned_stage(ctx, hbytes, &host, &ev_host)) != DTB_OK) return s;
+  // Everything of this call follows s_in: it starts after the caller's earlier work on `stream` and, when this
+  // set of staging and scratch served an earlier call, after that call's end.
+  DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pipe_start, stream));
+  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pipe_start, 0));
+  if (ctx->pset_used[set]) DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pset_free[set], 0));
   for (int k = 0; k < nchunks; ++k) {
     const uint64_t off = o_chunk[k] + L[k].o_hdr;
     std::memcpy(host + h_hoff + 8ull * k, &off, 8);
   }
-  DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_hoff, host + h_hoff, 8ull * nchunks, cudaMemcpyHostToDevice, stream));
+  DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_hoff, host + h_hoff, 8ull * nchunks, cudaMemcpyHostToDevice, ctx->s_in));
   for (int k = 0; k < nchunks; ++k) {
     std::vector<Job> cj(jobs.begin() + cut[k], jobs.begin() + cut[k + 1]);
     std::vector<uint8_t>& tab = ctx->hstage;
@@ -283,19 +294,14 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     std::copy(reinterpret_cast<const uint8_t*>(items[k].data()),
               reinterpret_cast<const uint8_t*>(items[k].data() + items[k].size()), host + h_items[k]);
     DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_chunk[k] + L[k].o_desc, host + h_tab[k], tab.size(), cudaMemcpyHostToDevice,
-                                  stream));
+                                  ctx->s_in));
     if (!items[k].empty())
       DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_items[k], host + h_items[k], sizeof(RepitchItem) * items[k].size(),
-                                    cudaMemcpyHostToDevice, stream));
+                                    cudaMemcpyHostToDevice, ctx->s_in));
   }
-  DTB_CUDA(ctx, cudaEventRecord(ev_host, stream));
-  cudaEvent_t ev_tables = event_at(ctx, 0);
-  if (!ev_tables) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
-  DTB_CUDA(ctx, cudaEventRecord(ev_tables, stream));
+  DTB_CUDA(ctx, cudaEventRecord(ev_host, ctx->s_in));
 
-  // ---- the pipeline ----
-  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ev_tables, 0));  // staging memory is free once earlier work is done
-  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pipe_done, 0));  // ... including the previous call's copies out
+  // ---- the pipeline: copies in, tile runs on the two lanes, copies out ----
   for (int k = 0; k < nchunks; ++k) {
     for (const Copy& c : cin[k])
       if ((s = issue(ctx, c, stage, true, ctx->s_in)) != DTB_OK) return s;
@@ -303,13 +309,12 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     if (!e_in) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
     DTB_CUDA(ctx, cudaEventRecord(e_in, ctx->s_in));
   }
-  DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_lane, ev_tables, 0));
   const int lanes = nchunks > 1 ? 2 : 1;
   LaunchTuning lane_tuning = tuning;
   lane_tuning.grid_percent = std::max(1, tuning.grid_percent / lanes);
   for (int k = 0; k < nchunks; ++k) {
     uint8_t* cbase = scratch + o_chunk[k];
-    cudaStream_t lane = (k % lanes) ? ctx->s_lane : stream;
+    cudaStream_t lane = (k % lanes) ? ctx->s_lane : ctx->s_lane0;
     DTB_CUDA(ctx, cudaStreamWaitEvent(lane, event_at(ctx, 1 + 3 * k), 0));
     if (!items[k].empty()) {
       const uint32_t blocks = std::min<uint32_t>((rows[k] + 7) / 8, (uint32_t)ctx->num_sms * 8);
@@ -328,14 +333,15 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   // Fold the chunks' status into the context's accumulator, then mark the call's end.
   pipe_fold<<<1, 32, 0, ctx->s_out>>>(scratch, reinterpret_cast<const uint64_t*>(scratch + o_hoff), nchunks, ctx->dpipe);
   DTB_CUDA(ctx, cudaGetLastError());
+  DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pset_free[set], ctx->s_out));
+  ctx->pset_used[set] = true;
   DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pipe_done, ctx->s_out));
-  DTB_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_pipe_done, 0));
   ctx->pipe_tiles += total_all;
   ctx->pipe_chunks += (uint64_t)nchunks;
   ctx->pipe_pending = true;
-  ctx->pipe_stream = stream;
   ctx->async_pending = false;
   if (flags & DTB_FLAG_ASYNC) return DTB_OK;  // dtb_sync(ctx, stream) waits and reports
+  DTB_CUDA(ctx, cudaStreamWaitEvent(stream, ctx->ev_pipe_done, 0));
   DTB_CUDA(ctx, cudaStreamSynchronize(stream));
   return finish_pipeline(ctx);
 }

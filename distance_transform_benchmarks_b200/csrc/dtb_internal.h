@@ -118,10 +118,20 @@ struct dtb_context_s {
   dtb::QueueHdr* dpipe = nullptr;
   cudaEvent_t ev_pipe_done = nullptr;
   bool pipe_pending = false;
-  cudaStream_t pipe_stream = nullptr;
   uint64_t pipe_tiles = 0, pipe_chunks = 0;
-  // Host-buffer pipeline: copy streams, a second compute lane, events, chunk size in pixels.
-  cudaStream_t s_in = nullptr, s_out = nullptr, s_lane = nullptr;
+  // Host-buffer pipeline: two sets of device staging + chunk scratch used by alternate calls, so that a call's
+  // copies in overlap the previous call's copies out; set i is free once ev_pset_free[i] (its last call's end)
+  // has completed.
+  void* pstage[2] = {nullptr, nullptr};
+  size_t pstage_size[2] = {0, 0};
+  void* pscratch[2] = {nullptr, nullptr};
+  size_t pscratch_size[2] = {0, 0};
+  cudaEvent_t ev_pset_free[2] = {nullptr, nullptr};
+  bool pset_used[2] = {false, false};
+  int pset_cur = 0;
+  cudaEvent_t ev_pipe_start = nullptr;
+  // Host-buffer pipeline: copy streams, two compute lanes, events, chunk size in pixels.
+  cudaStream_t s_in = nullptr, s_out = nullptr, s_lane = nullptr, s_lane0 = nullptr;
   std::vector<cudaEvent_t> evpool;
   uint64_t host_chunk_px = 16ull << 20;
   // dtb_gdt_ref_blocks: per-tile round counters of the running call (device scratch of `total` int32).
@@ -166,7 +176,8 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_ima
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
 // All images, masks and distances in host memory (ns-mode): chunked pipeline of 1-D host-to-device copies,
 // repitch, tile runs and 1-D device-to-host copies on overlapping streams.
-// DTB_FLAG_ASYNC: returns after enqueueing; dtb_sync reports the status of all such calls since the last one.
+// The call starts after the work enqueued on `stream` before it.  DTB_FLAG_ASYNC: returns after enqueueing,
+// without making `stream` wait for the call; dtb_sync waits for all such calls and reports their status.
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
                              const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags,
                              cudaStream_t stream);

@@ -55,10 +55,12 @@ typedef struct dtb_context_s* dtb_context;
 
 /* Flags (bitwise or). */
 #define DTB_FLAG_ASYNC 0x1u       /* return after enqueueing; dtb_sync() waits and reports the status.  For images in
-                                     device memory, and for ns-mode batches whose images, masks and maps are all in
-                                     host memory (those must stay valid and untouched until dtb_sync returns; the
-                                     status covers every such call since the last dtb_sync).  Other host-memory
-                                     calls ignore the flag. */
+                                     device memory (the work is ordered on `stream`), and for ns-mode batches whose
+                                     images, masks and maps are all in host memory: such a call starts after the
+                                     work enqueued on `stream` before it, but `stream` does not wait for its end
+                                     (successive calls overlap their copies); its buffers must stay valid and
+                                     untouched until dtb_sync returns, and the status covers every such call since
+                                     the last dtb_sync.  Other host-memory calls ignore the flag. */
 #define DTB_FLAG_ROUNDS 0x2u      /* plain per-image path: host-driven rounds over active tiles */
 #define DTB_FLAG_REF_NO_FMA 0x4u  /* ref-mode: round l_eucl*d and l_grad*|dI| separately instead of contracting */
 #define DTB_FLAG_TIMING 0x8u      /* record CUDA events around the tile kernel; dtb_stats.kernel_ms */
@@ -85,7 +87,8 @@ DTB_API void dtb_context_destroy(dtb_context ctx);
 /* Detailed text of the last error of this context ("" if none). */
 DTB_API const char* dtb_context_message(dtb_context ctx);
 DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out);
-/* Waits for work enqueued with DTB_FLAG_ASYNC on `stream` and returns its device status. */
+/* Waits for work enqueued with DTB_FLAG_ASYNC on `stream` and for every asynchronous host-buffer batch of the
+ * context, and returns their device status. */
 DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
 
 /* Launch tuning of the ns-mode tile kernel (chosen by dtb_plan_autotune, or set by hand).

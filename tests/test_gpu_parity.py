@@ -244,7 +244,7 @@ def test_host_pipeline_arena_runs(chunk_kpx):
 
 
 def test_host_pipeline_asynchronous_calls():
-    """Back-to-back asynchronous host batches (the next call's copies wait for the previous call's) and one
+    """Back-to-back asynchronous host batches (a call's copies in overlap the previous call's copies out) and one
     dtb_sync for all of them; a stalled call among them is reported by that sync, and the context recovers."""
     c = dtb.Context(0)
     c.set_tuning(host_chunk_kpx=64)
@@ -270,6 +270,32 @@ def test_host_pipeline_asynchronous_calls():
     dtb.geodesic_distance_transform_batch(iv, mv, gam, dists=dv, ctx=c)
     for k, (img, mask, g) in enumerate(batches[0]):
         assert_images_eq(dv[k], orc.ggdt_ns(img, mask, g), "after stall, image %d" % k)
+    c.close()
+
+
+def test_host_pipeline_alternate_buffer_sets():
+    """Successive host-buffer calls use alternate sets of device staging: calls of growing size (each set grows
+    while the other may be in flight), with a device-resident call and a synchronous host call between
+    asynchronous ones, all correct after one sync."""
+    c = dtb.Context(0)
+    c.set_tuning(host_chunk_kpx=32)
+    batches = [wl.config3(seed=40 + k, n=5 + 3 * k, smin=16, smax=120 + 60 * k) for k in range(5)]
+    arenas = [dtb.host_batch_arena([i for i, _, _ in b], [m for _, m, _ in b]) for b in batches]
+    dev_batch = wl.config3(seed=49, n=4, smin=30, smax=150)
+    dev_out = None
+    for k, (b, (iv, mv, dv)) in enumerate(zip(batches, arenas)):
+        sync_call = k == 3
+        dtb.geodesic_distance_transform_batch(iv, mv, [g for _, _, g in b], dists=dv, ctx=c, asynchronous=not sync_call)
+        if k == 1:
+            dev_out = dtb.geodesic_distance_transform_batch([cuda(i) for i, _, _ in dev_batch],
+                                                            [cuda(m) for _, m, _ in dev_batch],
+                                                            [g for _, _, g in dev_batch], ctx=c)
+    c.sync()
+    for j, (b, (_, _, dv)) in enumerate(zip(batches, arenas)):
+        for k, (img, mask, g) in enumerate(b):
+            assert_images_eq(dv[k], orc.ggdt_ns(img, mask, g), "call %d image %d" % (j, k))
+    for k, ((img, mask, g), d) in enumerate(zip(dev_batch, dev_out)):
+        assert_images_eq(d, orc.ggdt_ns(img, mask, g), "device call image %d" % k)
     c.close()
 
 
