@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--serve-requests", type=int, default=5000)
     p.add_argument("--serve-rate", type=float, default=500.0, help="Poisson arrival rate (requests / s)")
+    p.add_argument("--serve-saturated", type=int, default=1000,
+                   help="requests of the same mix submitted at once after the paced phase (capacity)")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-ref-mode", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the single-image C0 / C1 / C2 leg")
@@ -274,15 +276,12 @@ def run_serve(args, dev):
     kinds = rng.random(n) < 0.6
     live = []          # (image id, pool index) of images created so far
     pool_of = {}
-    lat, px, submitted = [], 0, 0
     next_id = 0
-    t0 = time.perf_counter()
-    for k in range(n):
-        while time.perf_counter() - t0 < arrivals[k]:
-            for c in srv.poll(wait_ms=0):
-                lat.append(c["latency_ms"])
-            time.sleep(0.0002)
-        if kinds[k] or not live:
+
+    def submit(new_image):
+        """One request of the mix; returns its pixels."""
+        nonlocal next_id
+        if new_image or not live:
             p = next_id % SERVE_POOL
             img, mask, g, out = pool[p]
             srv.submit_image(next_id, img, mask, g, out)
@@ -295,15 +294,44 @@ def run_serve(args, dev):
             hh, ww = img.shape[:2]
             disks = [(int(rng.integers(0, ww)), int(rng.integers(0, hh)), 3) for _ in range(int(rng.integers(1, 4)))]
             srv.submit_edit(iid, disks, out)
-        px += int(img.shape[0]) * int(img.shape[1])
+        return int(img.shape[0]) * int(img.shape[1])
+
+    def drain(lat, count, deadline):
+        while len(lat) < count:
+            for c in srv.poll(wait_ms=100):
+                lat.append(c["latency_ms"])
+            if time.perf_counter() > deadline:
+                break
+
+    lat, px, submitted = [], 0, 0
+    t0 = time.perf_counter()
+    for k in range(n):
+        while time.perf_counter() - t0 < arrivals[k]:
+            for c in srv.poll(wait_ms=0):
+                lat.append(c["latency_ms"])
+            time.sleep(0.0002)
+        px += submit(kinds[k])
         submitted += 1
-    while len(lat) < submitted:
-        for c in srv.poll(wait_ms=100):
-            lat.append(c["latency_ms"])
-        if time.perf_counter() - t0 > arrivals[-1] + 120:
-            break
+    drain(lat, submitted, t0 + arrivals[-1] + 120)
     elapsed = time.perf_counter() - t0
     st = srv.stats()
+    # Saturated phase: the same mix submitted at once; throughput = the engine's capacity.
+    ns = args.serve_saturated
+    saturated = None
+    if ns > 0:
+        lat2, px2 = [], 0
+        t1 = time.perf_counter()
+        for k in range(ns):
+            px2 += submit(rng.random() < 0.6)
+        drain(lat2, ns, t1 + 300)
+        el2 = time.perf_counter() - t1
+        st2 = srv.stats()
+        lat2 = np.array(lat2)
+        saturated = {"requests": ns, "completed": len(lat2), "failed": int(st2["failed"] - st["failed"]),
+                     "throughput_rps": len(lat2) / el2, "mpx_s": px2 / 1e6 / el2,
+                     "waves": int(st2["waves"] - st["waves"]), "p50_ms": float(np.percentile(lat2, 50)),
+                     "p99_ms": float(np.percentile(lat2, 99)),
+                     "note": "all requests submitted at t=0 (latency includes queueing behind earlier requests)"}
     srv.close()
     lat = np.array(lat)
     return {"requests": n, "rate_rps": args.serve_rate, "new_fraction": 0.6, "completed": int(st["completed"]),
@@ -311,7 +339,8 @@ def run_serve(args, dev):
             "mean_ms": float(lat.mean()), "throughput_rps": len(lat) / elapsed, "mpx_s": px / 1e6 / elapsed,
             "waves": int(st["waves"]), "requests_per_wave": len(lat) / max(1, st["waves"]),
             "hbm_budget_gb": SERVE_BUDGET / 2 ** 30, "evictions": int(st["evictions"]),
-            "images": "sides log-U[256,4096], half gray blobs / half rgb8 Voronoi, %d distinct" % SERVE_POOL}
+            "images": "sides log-U[256,4096], half gray blobs / half rgb8 Voronoi, %d distinct" % SERVE_POOL,
+            "saturated": saturated}
 
 
 def run_reference(args, dist):

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -166,6 +167,17 @@ size_t plane_pitch(size_t row_bytes) { return row_bytes % 16 ? align_up(row_byte
 
 }  // namespace
 
+// Device and pinned host buffers of one wave in flight; a slot is reused only after its previous wave ended.
+struct WaveSlot {
+  void* scratch = nullptr;  // queue, tile states, tables of the wave
+  size_t scratch_size = 0;
+  void* stage = nullptr;    // packed staging of new images whose rows need a pitch change
+  size_t stage_size = 0;
+  uint8_t* hpin = nullptr;  // pinned host copy of the wave's tables
+  size_t hpin_size = 0;
+  cudaEvent_t ev_in = nullptr, ev_comp = nullptr, ev_done = nullptr;
+};
+
 struct dtb_server_s {
   dtb_context ctx = nullptr;
   dtb_serve_config cfg{};
@@ -181,12 +193,9 @@ struct dtb_server_s {
   int64_t next_rid = 1;
   uint64_t tick = 0;
   int64_t wave_no = 0;
-  void* wscratch = nullptr;
-  size_t wscratch_size = 0;
-  void* wstage = nullptr;
-  size_t wstage_size = 0;
-  std::vector<uint8_t> host;
-  cudaStream_t stream = nullptr;
+  int64_t busy_from = 1;  // residents with wave >= busy_from belong to a wave in flight
+  WaveSlot slot[2];
+  cudaStream_t s_in = nullptr, s_run = nullptr, s_out = nullptr;  // copies in, tile runs, copies out
   dtb_serve_stats st{};
 };
 
@@ -215,7 +224,7 @@ bool make_room(dtb_server s, size_t bytes, size_t* off) {
     uint64_t oldest = UINT64_MAX;
     bool found = false;
     for (auto& kv : s->resident) {
-      if (kv.second.wave == s->wave_no || referenced(s, kv.first)) continue;
+      if (kv.second.wave >= s->busy_from || referenced(s, kv.first)) continue;
       if (kv.second.last_use < oldest) {
         oldest = kv.second.last_use;
         victim = kv.first;
@@ -249,8 +258,8 @@ std::vector<Request> admit(dtb_server s) {
         complete(s, q, DTB_ERR_INVALID_ARG, now);  // not resident (never submitted, released or evicted)
         continue;
       }
-      if (it->second.wave == s->wave_no) {
-        keep.push_back(std::move(q));  // one request per image per wave
+      if (it->second.wave >= s->busy_from) {
+        keep.push_back(std::move(q));  // one wave in flight per image: its map may still be on its way out
         continue;
       }
       it->second.wave = s->wave_no;
@@ -299,9 +308,23 @@ std::vector<Request> admit(dtb_server s) {
   return wave;
 }
 
-dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
+// A wave in flight: its requests, slot and device queue header.
+struct InFlight {
+  std::vector<Request> reqs;
+  int slot = 0;
+  int64_t no = 0;
+  uint32_t total = 0;
+  const QueueHdr* hdr = nullptr;
+};
+
+// Enqueues one wave: copies in and table upload on s_in, tile work on s_run, copies out on s_out; ev_done of
+// the slot marks its end.  Requests of the wave reference no image of another wave in flight (admit), so the
+// waves' device work only shares the arena's free space and the tile-run stream.
+dtb_status launch_wave(dtb_server s, InFlight& f) {
   dtb_context ctx = s->ctx;
-  cudaStream_t st = s->stream;
+  cudaStream_t st = s->s_run;
+  WaveSlot& ws = s->slot[f.slot];
+  std::vector<Request>& wave = f.reqs;
   const int n = (int)wave.size();
   std::vector<Resident*> rs(n);
   {
@@ -347,9 +370,9 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
       }
     }
   }
-  dtb_status s2 = grow(ctx, &s->wstage, &s->wstage_size, std::max<size_t>(stage_bytes, 256));
+  dtb_status s2 = grow(ctx, &ws.stage, &ws.stage_size, std::max<size_t>(stage_bytes, 256));
   if (s2 != DTB_OK) return s2;
-  uint8_t* stage = static_cast<uint8_t*>(s->wstage);
+  uint8_t* stage = static_cast<uint8_t*>(ws.stage);
   // Host -> device: one 1-D copy per plane (into the resident plane, or into staging + repitch).
   for (int i = 0; i < n; ++i) {
     if (warm[i]) continue;
@@ -359,13 +382,13 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
     uint8_t* dimg = o_stage_img[i] == SIZE_MAX ? const_cast<uint8_t*>(jobs[i].img) : stage + o_stage_img[i];
     uint8_t* dmask = o_stage_mask[i] == SIZE_MAX ? const_cast<uint8_t*>(jobs[i].mask) : stage + o_stage_mask[i];
     if ((size_t)q.img.pitch == rb)
-      DTB_CUDA(ctx, cudaMemcpyAsync(dimg, q.img.buffer, rb * r.H, cudaMemcpyHostToDevice, st));
+      DTB_CUDA(ctx, cudaMemcpyAsync(dimg, q.img.buffer, rb * r.H, cudaMemcpyHostToDevice, s->s_in));
     else
-      DTB_CUDA(ctx, cudaMemcpy2DAsync(dimg, rb, q.img.buffer, q.img.pitch, rb, r.H, cudaMemcpyHostToDevice, st));
+      DTB_CUDA(ctx, cudaMemcpy2DAsync(dimg, rb, q.img.buffer, q.img.pitch, rb, r.H, cudaMemcpyHostToDevice, s->s_in));
     if (q.mask.pitch == r.W)
-      DTB_CUDA(ctx, cudaMemcpyAsync(dmask, q.mask.buffer, (size_t)r.W * r.H, cudaMemcpyHostToDevice, st));
+      DTB_CUDA(ctx, cudaMemcpyAsync(dmask, q.mask.buffer, (size_t)r.W * r.H, cudaMemcpyHostToDevice, s->s_in));
     else
-      DTB_CUDA(ctx, cudaMemcpy2DAsync(dmask, r.W, q.mask.buffer, q.mask.pitch, r.W, r.H, cudaMemcpyHostToDevice, st));
+      DTB_CUDA(ctx, cudaMemcpy2DAsync(dmask, r.W, q.mask.buffer, q.mask.pitch, r.W, r.H, cudaMemcpyHostToDevice, s->s_in));
     if (o_stage_img[i] != SIZE_MAX) {
       items.push_back({dimg, const_cast<uint8_t*>(jobs[i].img), (uint32_t)rb, (uint32_t)r.H, (uint32_t)r.img_pitch, rows});
       rows += (uint32_t)r.H;
@@ -387,18 +410,35 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
   off = align_up(off + sizeof(DiskItem) * std::max<size_t>(disks.size(), 1), 256);
   const size_t o_items = off;
   off = align_up(off + sizeof(RepitchItem) * std::max<size_t>(items.size(), 1), 256);
-  if ((s2 = grow(ctx, &s->wscratch, &s->wscratch_size, off)) != DTB_OK) return s2;
-  uint8_t* sc = static_cast<uint8_t*>(s->wscratch);
+  if ((s2 = grow(ctx, &ws.scratch, &ws.scratch_size, off)) != DTB_OK) return s2;
+  uint8_t* sc = static_cast<uint8_t*>(ws.scratch);
   std::vector<uint8_t> tab;
   if ((s2 = build_tables(ctx, jobs, L, tab)) != DTB_OK) return s2;
-  s->host.assign(off - L.o_desc, 0);
-  std::copy(tab.begin(), tab.end(), s->host.begin());
-  std::copy(warm.begin(), warm.end(), s->host.begin() + (o_warm - L.o_desc));
+  // Tables, warm flags, disks and repitch items: one upload from the slot's pinned buffer (free: the slot's
+  // previous wave has ended), so that the copy does not wait for the other wave's work.
+  const size_t hbytes = off - L.o_desc;
+  if (ws.hpin_size < hbytes) {
+    if (ws.hpin) cudaFreeHost(ws.hpin);
+    ws.hpin = nullptr;
+    ws.hpin_size = 0;
+    const size_t sz = align_up(hbytes + hbytes / 4, 1 << 16);
+    if (cudaHostAlloc((void**)&ws.hpin, sz, cudaHostAllocDefault) != cudaSuccess) {
+      ws.hpin = nullptr;
+      return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "cudaHostAlloc(serve tables) failed");
+    }
+    ws.hpin_size = sz;
+  }
+  uint8_t* host = ws.hpin;
+  std::memset(host, 0, hbytes);
+  std::copy(tab.begin(), tab.end(), host);
+  std::copy(warm.begin(), warm.end(), host + (o_warm - L.o_desc));
   std::copy(reinterpret_cast<const uint8_t*>(disks.data()), reinterpret_cast<const uint8_t*>(disks.data() + disks.size()),
-            s->host.begin() + (o_disks - L.o_desc));
+            host + (o_disks - L.o_desc));
   std::copy(reinterpret_cast<const uint8_t*>(items.data()), reinterpret_cast<const uint8_t*>(items.data() + items.size()),
-            s->host.begin() + (o_items - L.o_desc));
-  DTB_CUDA(ctx, cudaMemcpyAsync(sc + L.o_desc, s->host.data(), s->host.size(), cudaMemcpyHostToDevice, st));
+            host + (o_items - L.o_desc));
+  DTB_CUDA(ctx, cudaMemcpyAsync(sc + L.o_desc, host, hbytes, cudaMemcpyHostToDevice, s->s_in));
+  DTB_CUDA(ctx, cudaEventRecord(ws.ev_in, s->s_in));
+  DTB_CUDA(ctx, cudaStreamWaitEvent(st, ws.ev_in, 0));
   const dtb_status qs = reset_queue(ctx, sc, L, st);
   if (qs != DTB_OK) return qs;
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(sc + L.o_desc);
@@ -406,6 +446,8 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
   const uint32_t* dbase = reinterpret_cast<const uint32_t*>(sc + L.o_base);
   uint32_t* states = reinterpret_cast<uint32_t*>(sc + L.o_states);
   Queue q = make_queue(sc, L);
+  f.hdr = total > 0 ? reinterpret_cast<QueueHdr*>(sc + L.o_hdr) : nullptr;
+  f.total = total;
   if (!items.empty()) {
     repitch_rows<<<std::min<uint32_t>((rows + 7) / 8, (uint32_t)ctx->num_sms * 8), 256, 0, st>>>(
         reinterpret_cast<const RepitchItem*>(sc + o_items), (int)items.size(), rows);
@@ -440,57 +482,131 @@ dtb_status run_wave(dtb_server s, std::vector<Request>& wave) {
     ggdt_finalize<<<blocks, 128, 0, st>>>(ddesc, dbase, n, total, states);
     DTB_CUDA(ctx, cudaGetLastError());
   }
+  DTB_CUDA(ctx, cudaEventRecord(ws.ev_comp, st));
   // Device -> host: each request's map into its output buffer.
+  DTB_CUDA(ctx, cudaStreamWaitEvent(s->s_out, ws.ev_comp, 0));
   for (int i = 0; i < n; ++i) {
     const dtb_image& o = wave[i].r.out;
     if (o.width == 0 || o.height == 0) continue;
     DTB_CUDA(ctx, cudaMemcpy2DAsync(o.buffer, o.pitch, jobs[i].dist, jobs[i].dist_pitch, 4 * (size_t)o.width, o.height,
-                                    cudaMemcpyDeviceToHost, st));
+                                    cudaMemcpyDeviceToHost, s->s_out));
   }
-  DTB_CUDA(ctx, cudaStreamSynchronize(st));
-  dtb_stats ds{};
-  const dtb_status status = read_device_status(ctx, reinterpret_cast<QueueHdr*>(sc + L.o_hdr), &ds);
-  s->st.tile_visits += ds.tile_visits;
-  s->st.tiles += total;
-  return status;
+  DTB_CUDA(ctx, cudaEventRecord(ws.ev_done, s->s_out));
+  return DTB_OK;
 }
 
+// Completes the requests of a wave that has ended (or failed to enqueue): a failed new image is dropped, since
+// its map is not valid.  Caller holds mu.
+void retire_wave(dtb_server s, InFlight& f, dtb_status status) {
+  const auto now = Clock::now();
+  s->st.waves += 1;
+  for (const Request& q : f.reqs) {
+    if (status != DTB_OK && q.r.kind == DTB_REQ_IMAGE) {
+      auto it = s->resident.find(q.r.image_id);
+      if (it != s->resident.end()) {
+        s->arena.release(it->second.off, it->second.bytes);
+        s->resident.erase(it);
+      }
+    }
+    complete(s, q, status, now);
+  }
+}
+
+// The worker keeps up to two waves in flight: while one runs, the next is admitted and enqueued, so its copies
+// in and host preparation overlap the running tile kernel, and its tile kernel overlaps the previous wave's
+// copies out.  A request whose image belongs to a wave in flight waits for that wave's end (admit).
 void worker_main(dtb_server s) {
   cudaSetDevice(s->ctx->device);
+  std::deque<InFlight> inflight;
+  int next_slot = 0;
+  int64_t blocked_at = -1;  // submissions counted when an admission found nothing to run beside a wave in flight
+  auto set_busy_from = [&] { s->busy_from = inflight.empty() ? s->wave_no + 1 : inflight.front().no; };
   for (;;) {
-    std::vector<Request> wave;
+    InFlight f;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_sub.wait(lk, [&] { return s->stop || !s->pending.empty(); });
-      if (s->stop && s->pending.empty()) break;
-      ++s->wave_no;
-      wave = admit(s);
-      if (wave.empty()) {
-        s->cv_done.notify_all();
-        if (!s->pending.empty()) {
-          // nothing fits right now and nothing runs: the head request can never fit
-          complete(s, s->pending.front(), DTB_ERR_CAPACITY, Clock::now());
-          s->pending.pop_front();
+      if (inflight.empty()) s->cv_sub.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+      if (inflight.empty() && s->stop && s->pending.empty()) break;
+      if (inflight.size() < 2 && !s->pending.empty() && s->st.submitted != blocked_at) {
+        f.no = ++s->wave_no;
+        s->busy_from = inflight.empty() ? f.no : inflight.front().no;  // during admission and while f runs
+        f.reqs = admit(s);
+        if (f.reqs.empty()) {
+          set_busy_from();
+          s->cv_done.notify_all();  // admission may have completed invalid requests
+          if (inflight.empty()) {
+            // nothing fits and nothing runs: the head request can never fit
+            if (!s->pending.empty()) {
+              complete(s, s->pending.front(), DTB_ERR_CAPACITY, Clock::now());
+              s->pending.pop_front();
+            }
+            continue;
+          }
+          blocked_at = s->st.submitted;  // retry after the oldest wave ends or a request arrives
         }
+      }
+    }
+    if (!f.reqs.empty()) {
+      f.slot = next_slot;
+      next_slot ^= 1;
+      const dtb_status ls = launch_wave(s, f);
+      if (ls != DTB_OK) {
+        // Nothing of this wave may still run when its requests complete.
+        cudaStreamSynchronize(s->s_in);
+        cudaStreamSynchronize(s->s_run);
+        cudaStreamSynchronize(s->s_out);
+        std::lock_guard<std::mutex> lk(s->mu);
+        retire_wave(s, f, ls);
+        set_busy_from();
+        s->cv_done.notify_all();
         continue;
       }
+      inflight.push_back(std::move(f));
+      continue;
     }
-    const dtb_status status = run_wave(s, wave);
-    const auto now = Clock::now();
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->st.waves += 1;
-    for (const Request& q : wave) {
-      if (status != DTB_OK && q.r.kind == DTB_REQ_IMAGE) {
-        auto it = s->resident.find(q.r.image_id);  // its map is not valid: drop the image
-        if (it != s->resident.end()) {
-          s->arena.release(it->second.off, it->second.bytes);
-          s->resident.erase(it);
+    // Nothing to enqueue now: wait for the oldest wave's end or, with a slot free, for a new request.
+    InFlight& old = inflight.front();
+    cudaEvent_t ev = s->slot[old.slot].ev_done;
+    if (inflight.size() < 2) {
+      bool ended = false;
+      for (;;) {
+        if (cudaEventQuery(ev) != cudaErrorNotReady) {
+          ended = true;
+          break;
         }
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->st.submitted != blocked_at && !s->pending.empty()) break;
+        s->cv_sub.wait_for(lk, std::chrono::microseconds(50));
       }
-      complete(s, q, status, now);
+      if (!ended) continue;
     }
+    dtb_status status = cudaEventSynchronize(ev) == cudaSuccess ? DTB_OK : DTB_ERR_CUDA;
+    dtb_stats ds{};
+    if (status == DTB_OK && old.hdr) status = read_device_status(s->ctx, old.hdr, &ds);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->st.tile_visits += ds.tile_visits;
+    s->st.tiles += old.total;
+    retire_wave(s, old, status);
+    inflight.pop_front();
+    set_busy_from();
+    blocked_at = -1;
     s->cv_done.notify_all();
   }
+}
+
+// Frees the server's device and host resources (no wave in flight).
+void release_server(dtb_server s) {
+  for (WaveSlot& w : s->slot) {
+    if (w.scratch) cudaFree(w.scratch);
+    if (w.stage) cudaFree(w.stage);
+    if (w.hpin) cudaFreeHost(w.hpin);
+    for (cudaEvent_t e : {w.ev_in, w.ev_comp, w.ev_done})
+      if (e) cudaEventDestroy(e);
+  }
+  for (cudaStream_t t : {s->s_in, s->s_run, s->s_out})
+    if (t) cudaStreamDestroy(t);
+  if (s->arena_base) cudaFree(s->arena_base);
+  delete s;
 }
 
 }  // namespace
@@ -514,9 +630,15 @@ DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg
     return DTB_ERR_OUT_OF_MEMORY;
   }
   s->arena.reset(cfg->hbm_budget_bytes);
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaFree(s->arena_base);
-    delete s;
+  bool ok = cudaStreamCreateWithFlags(&s->s_in, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&s->s_run, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking) == cudaSuccess;
+  for (WaveSlot& w : s->slot)
+    ok = ok && cudaEventCreateWithFlags(&w.ev_in, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&w.ev_comp, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&w.ev_done, cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    release_server(s);
     return DTB_ERR_CUDA;
   }
   s->worker = std::thread(worker_main, s);
@@ -578,7 +700,7 @@ DTB_API dtb_status dtb_serve_release(dtb_server s, int64_t image_id) {
   if (!s) return DTB_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->resident.find(image_id);
-  if (it == s->resident.end() || it->second.wave == s->wave_no || referenced(s, image_id)) return DTB_ERR_INVALID_ARG;
+  if (it == s->resident.end() || it->second.wave >= s->busy_from || referenced(s, image_id)) return DTB_ERR_INVALID_ARG;
   s->arena.release(it->second.off, it->second.bytes);
   s->resident.erase(it);
   return DTB_OK;
@@ -604,11 +726,7 @@ DTB_API void dtb_serve_destroy(dtb_server s) {
   }
   s->cv_sub.notify_all();
   if (s->worker.joinable()) s->worker.join();
-  if (s->stream) cudaStreamDestroy(s->stream);
-  if (s->arena_base) cudaFree(s->arena_base);
-  if (s->wscratch) cudaFree(s->wscratch);
-  if (s->wstage) cudaFree(s->wstage);
-  delete s;
+  release_server(s);
 }
 
 }  // extern "C"

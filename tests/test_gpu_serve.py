@@ -113,3 +113,39 @@ def test_budget_eviction_and_capacity():
     rid = srv.submit_image(99, torch.from_numpy(big), torch.from_numpy(big), 0.1, out)
     assert _drain(srv, 1)[rid]["status"] == 7
     srv.close()
+
+
+def test_overlapping_small_waves_keep_per_image_order():
+    """Two waves in flight at a time: with at most two requests per wave, new images and edits of images whose
+    own wave may still be running (they wait for it) are all exact, edits applied in submission order."""
+    rng = np.random.default_rng(7)
+    batch = _images(33, 24, smin=40, smax=260)
+    srv = dtb.Server(512 << 20, max_wave_requests=2)
+    masks_now, outs, expected = {}, {}, {}
+
+    def edit(j):
+        img, _, g = batch[j]
+        disks = _disks(rng, img, int(rng.integers(1, 4)))
+        masks_now[j] = _mask_with(masks_now[j], disks)
+        out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+        rid = srv.submit_edit(j, disks, out)
+        outs[rid] = out
+        expected[rid] = orc.ggdt_ns(img, masks_now[j], g)
+
+    for i, (img, mask, g) in enumerate(batch):
+        out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+        rid = srv.submit_image(i, torch.from_numpy(img).pin_memory(), torch.from_numpy(mask).pin_memory(), g, out)
+        outs[rid] = out
+        expected[rid] = orc.ggdt_ns(img, mask, g)
+        masks_now[i] = mask.copy()
+        if i % 3 == 2:
+            for j in (i, i, i - 2):
+                edit(j)
+    got = _drain(srv, len(outs))
+    for rid, c in got.items():
+        assert c["status"] == 0, c
+        assert_images_eq(outs[rid], expected[rid], "request %d" % rid)
+    st = srv.stats()
+    assert st["completed"] == len(outs) and st["failed"] == 0
+    assert st["waves"] >= len(outs) // 2
+    srv.close()
