@@ -132,10 +132,20 @@ __global__ void __launch_bounds__(256) ggdt_add_counts(int32_t* __restrict__ cou
 // workers idle in queue_pop until the no-progress watchdog sets DERR_QUEUE_TIMEOUT and every worker returns.
 __global__ void ggdt_phantom_pending(QueueHdr* hdr) { atomicAdd(&hdr->pending.v, 1u); }
 
-// Tiles never reached keep uninitialised memory: write v there.
+// Tiles never reached keep uninitialised memory: write v there.  With `fold`, one thread also adds the run's
+// queue header `hdr` into the accumulator `fold` (first error kept, counters summed): runs of the host-buffer
+// pipeline report their status this way, on their own stream, without a separate kernel.
 __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
-                                                     int n, uint32_t total, const uint32_t* __restrict__ states) {
+                                                     int n, uint32_t total, const uint32_t* __restrict__ states,
+                                                     const QueueHdr* hdr, QueueHdr* fold) {
   const int lane = threadIdx.x & 31;
+  if (fold && blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t err = hdr->error.v;
+    if (err != 0u && atomicCAS(&fold->error.v, 0u, err) == 0u) fold->err_info.v = hdr->err_info.v;
+    atomicAdd(&fold->progress.v, hdr->progress.v);
+    atomicAdd(&fold->phases.v, hdr->phases.v);
+    atomicAdd(&fold->activations.v, hdr->activations.v);
+  }
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t t = warp; t < total; t += nwarps) {
@@ -368,7 +378,7 @@ dtb_status reset_queue(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, 
 }
 
 dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
-                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1) {
+                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1, QueueHdr* fold) {
   const uint64_t stall_ns = ctx->inject_stall_ns;
   ctx->inject_stall_ns = 0;
   Queue q = make_queue(dbase, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS);
@@ -403,7 +413,7 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
   const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant] : (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
   DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, fn, args));
   if (ev1) DTB_CUDA(ctx, cudaEventRecord(ev1, stream));
-  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states);
+  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q.hdr, fold);
   DTB_CUDA(ctx, cudaGetLastError());
   return DTB_OK;
 }
@@ -457,7 +467,7 @@ static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayou
     if (err_prog[1] > q.max_visits)
       return fail(ctx, DTB_ERR_DEVICE, "visit limit exceeded after %llu rounds", (unsigned long long)*nrounds);
   }
-  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, L.n, total, states);
+  ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, L.n, total, states, nullptr, nullptr);
   DTB_CUDA(ctx, cudaGetLastError());
   return DTB_OK;
 }

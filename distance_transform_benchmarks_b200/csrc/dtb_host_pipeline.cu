@@ -50,22 +50,6 @@ __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restric
   }
 }
 
-// Folds the queue headers of a call's chunks into the context's accumulator: first error, counters summed.
-__global__ void pipe_fold(const uint8_t* __restrict__ scratch, const uint64_t* __restrict__ hdr_off, int nchunks,
-                          QueueHdr* acc) {
-  if (threadIdx.x != 0) return;
-  for (int k = 0; k < nchunks; ++k) {
-    const QueueHdr* h = reinterpret_cast<const QueueHdr*>(scratch + hdr_off[k]);
-    if (acc->error.v == 0 && h->error.v != 0) {
-      acc->error.v = h->error.v;
-      acc->err_info.v = h->err_info.v;
-    }
-    acc->progress.v += h->progress.v;
-    acc->phases.v += h->phases.v;
-    acc->activations.v += h->activations.v;
-  }
-}
-
 namespace {
 
 cudaEvent_t event_at(dtb_context ctx, size_t i) {
@@ -257,8 +241,6 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     o_items[k] = soff;
     soff = align_up(soff + sizeof(RepitchItem) * std::max<size_t>(items[k].size(), 1), 256);
   }
-  const size_t o_hoff = soff;  // chunk header offsets, for pipe_fold
-  soff = align_up(soff + 8ull * nchunks, 256);
   if ((s = grow(ctx, &ctx->pscratch[set], &ctx->pscratch_size[set], soff)) != DTB_OK) return s;
   uint8_t* scratch = static_cast<uint8_t*>(ctx->pscratch[set]);
   // Only the descriptor tables, tensor maps and repitch lists of each chunk go up (one pinned block, one copy
@@ -271,8 +253,6 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     h_items[k] = hbytes;
     hbytes += sizeof(RepitchItem) * items[k].size();
   }
-  const size_t h_hoff = hbytes;
-  hbytes += 8ull * nchunks;
   uint8_t* host = nullptr;
   cudaEvent_t ev_host = nullptr;
   if ((s = pinned_stage(ctx, hbytes, &host, &ev_host)) != DTB_OK) return s;
@@ -281,11 +261,6 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
   DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pipe_start, stream));
   DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pipe_start, 0));
   if (ctx->pset_used[set]) DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_in, ctx->ev_pset_free[set], 0));
-  for (int k = 0; k < nchunks; ++k) {
-    const uint64_t off = o_chunk[k] + L[k].o_hdr;
-    std::memcpy(host + h_hoff + 8ull * k, &off, 8);
-  }
-  DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_hoff, host + h_hoff, 8ull * nchunks, cudaMemcpyHostToDevice, ctx->s_in));
   for (int k = 0; k < nchunks; ++k) {
     std::vector<Job> cj(jobs.begin() + cut[k], jobs.begin() + cut[k + 1]);
     std::vector<uint8_t>& tab = ctx->hstage;
@@ -322,7 +297,8 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
                                             (int)items[k].size(), rows[k]);
       DTB_CUDA(ctx, cudaGetLastError());
     }
-    if ((s = enqueue_persistent(ctx, cbase, L[k], MODE_NS, lane_tuning, lane, nullptr, nullptr)) != DTB_OK) return s;
+    if ((s = enqueue_persistent(ctx, cbase, L[k], MODE_NS, lane_tuning, lane, nullptr, nullptr, ctx->dpipe)) != DTB_OK)
+      return s;
     cudaEvent_t e_run = event_at(ctx, 2 + 3 * k);
     if (!e_run) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
     DTB_CUDA(ctx, cudaEventRecord(e_run, lane));
@@ -330,9 +306,9 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     for (const Copy& c : cout[k])
       if ((s = issue(ctx, c, stage, false, ctx->s_out)) != DTB_OK) return s;
   }
-  // Fold the chunks' status into the context's accumulator, then mark the call's end.
-  pipe_fold<<<1, 32, 0, ctx->s_out>>>(scratch, reinterpret_cast<const uint64_t*>(scratch + o_hoff), nchunks, ctx->dpipe);
-  DTB_CUDA(ctx, cudaGetLastError());
+  // The call's end: its last copy out (each chunk's run, which folded its status into ctx->dpipe, came before
+  // that chunk's copy out).  Only copies run on s_out, so the next calls are not held up by a kernel waiting
+  // for SMs that the tile runs hold.
   DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pset_free[set], ctx->s_out));
   ctx->pset_used[set] = true;
   DTB_CUDA(ctx, cudaEventRecord(ctx->ev_pipe_done, ctx->s_out));

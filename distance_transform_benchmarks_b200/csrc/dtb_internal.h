@@ -169,9 +169,10 @@ dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* 
 // Resident warps of the tile kernel of `mode` under `t`.
 uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t);
 // Enqueues queue reset, seed scan, the persistent tile kernel and finalize on `stream` (capturable).
-// ev0 / ev1 (optional) are recorded around the tile kernel.
+// ev0 / ev1 (optional) are recorded around the tile kernel; `fold` (optional) receives the run's status and
+// counters, added by finalize.
 dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
-                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1);
+                              cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1, QueueHdr* fold = nullptr);
 dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_image* const* imgs,
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
 // All images, masks and distances in host memory (ns-mode): chunked pipeline of 1-D host-to-device copies,
@@ -188,7 +189,8 @@ dtb_status pinned_stage(dtb_context ctx, size_t need, uint8_t** out, cudaEvent_t
 
 // Kernels shared across translation units (defined in dtb_api.cu / dtb_host_pipeline.cu).
 __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__ descs, const uint32_t* __restrict__ tile_base,
-                                                     int n, uint32_t total, const uint32_t* __restrict__ states);
+                                                     int n, uint32_t total, const uint32_t* __restrict__ states,
+                                                     const QueueHdr* hdr, QueueHdr* fold);
 struct RepitchItem {
   const uint8_t* src;
   uint8_t* dst;

@@ -479,7 +479,7 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
     cfg.numAttrs = 1;
     void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
     DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->ns_fn[tuning.variant], args));
-    ggdt_finalize<<<blocks, 128, 0, st>>>(ddesc, dbase, n, total, states);
+    ggdt_finalize<<<blocks, 128, 0, st>>>(ddesc, dbase, n, total, states, nullptr, nullptr);
     DTB_CUDA(ctx, cudaGetLastError());
   }
   DTB_CUDA(ctx, cudaEventRecord(ws.ev_comp, st));
