@@ -416,3 +416,40 @@ def test_ref_runs_are_bit_identical_under_load(ctx):
     for rep in range(30):
         dtb.generalised_distance_transform(ti, tm, 0.5, dist=d, ctx=ctx)
         assert torch.equal(d, a), (rep, int((d != a).sum()))
+
+
+@pytest.mark.parametrize("kind,h,w,gamma", [("gray", 2048, 1536, 0.0), ("rgb8", 1500, 2100, 0.0),
+                                            ("const", 4096, 4096, 1.0)])
+def test_ns_unit_weights_are_city_block_distance(ctx, kind, h, w, gamma):
+    """Oracle-free check at sizes the CPU restatement is slow on: with every C4 edge weighing exactly 1
+    (gamma = 0, or an image without intensity steps) the map is the integer city-block distance to the nearest
+    seed, which scipy computes independently."""
+    from scipy import ndimage
+    rng = np.random.default_rng(17)
+    if kind == "const":
+        img = np.full((h, w), 77, np.uint8)
+    elif kind == "gray":
+        img = rng.integers(0, 256, (h, w), dtype=np.uint8)
+    else:
+        img = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+    mask = wl.random_disks(rng, w, h, 5, 1, 6)
+    d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=ctx)
+    expect = ndimage.distance_transform_cdt(mask == 0, metric="taxicab").astype(np.float32)
+    assert_images_eq(d, expect, "unit weights, %s %dx%d" % (kind, h, w))
+
+
+@pytest.mark.parametrize("which", ["config1", "config2"])
+def test_full_size_union_of_seed_sets_is_elementwise_min(ctx, which):
+    """The map is the minimum, over paths from any seed, of the path's fp32 sum, and a path's sum does not depend
+    on which other seeds exist: T(A | B) == min(T(A), T(B)) bit for bit, at the full sizes of the 4096^2 maze
+    and the 8192^2 rgb8 workload."""
+    img, mask_a, gamma = getattr(wl, which)()
+    h, w = mask_a.shape
+    mask_b = wl.random_disks(np.random.default_rng(23), w, h, 7, 2, 6)
+    ti = cuda(img)
+    da = dtb.geodesic_distance_transform(ti, cuda(mask_a), gamma, ctx=ctx)
+    db = dtb.geodesic_distance_transform(ti, cuda(mask_b), gamma, ctx=ctx)
+    du = dtb.geodesic_distance_transform(ti, cuda(mask_a | mask_b), gamma, ctx=ctx)
+    expect = torch.minimum(da, db)
+    assert torch.equal(du, expect), int((du != expect).sum())
+    assert ctx.stats()["device_error"] == 0

@@ -81,3 +81,35 @@ def test_no_seed_gives_v_everywhere():
     mask = np.zeros_like(img)
     assert np.all(orc.ggdt_ns(img, mask, 1.0, v=123.0) == np.float32(123.0))
     assert np.all(orc.ggdt_ref(img, mask, 0.5, v=7.0) == np.float32(7.0))
+
+
+@pytest.mark.parametrize("kind", ["gray", "rgb8", "const"])
+def test_ns_unit_weights_are_city_block_distance(kind):
+    """gamma = 0 (or an image without intensity steps) makes every C4 edge weigh exactly 1: the map is then the
+    integer city-block distance to the nearest seed, computed independently by scipy's chamfer transform."""
+    from scipy import ndimage
+    from distance_transform_benchmarks_b200 import workloads as wl
+    rng = np.random.default_rng(17)
+    h, w = 97, 131
+    if kind == "const":
+        img, gamma = np.full((h, w), 77, np.uint8), 1.0
+    elif kind == "gray":
+        img, gamma = rng.integers(0, 256, (h, w), dtype=np.uint8), 0.0
+    else:
+        img, gamma = rng.integers(0, 256, (h, w, 3), dtype=np.uint8), 0.0
+    mask = wl.random_disks(rng, w, h, 5, 1, 6)
+    expect = ndimage.distance_transform_cdt(mask == 0, metric="taxicab").astype(np.float32)
+    assert_images_eq(orc.ggdt_ns(img, mask, gamma), expect, "unit weights, %s" % kind)
+
+
+@pytest.mark.parametrize("rgb", [False, True])
+def test_ns_union_of_seed_sets_is_elementwise_min(rgb):
+    """A value is the minimum over paths of the path's fp32 sum from its seed: T(A | B) == min(T(A), T(B))."""
+    from distance_transform_benchmarks_b200 import workloads as wl
+    rng = np.random.default_rng(5)
+    img = wl.voronoi_rgb(3, 150, 120) if rgb else wl.blobs_gray(3, 150, 120)
+    a = wl.random_disks(rng, 150, 120, 3, 1, 4)
+    b = wl.random_disks(rng, 150, 120, 4, 1, 4)
+    for g in (0.02, 1.0):
+        expect = np.minimum(orc.ggdt_ns(img, a, g), orc.ggdt_ns(img, b, g))
+        assert_images_eq(orc.ggdt_ns(img, a | b, g), expect, "union, gamma %g" % g)
