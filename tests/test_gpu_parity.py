@@ -453,3 +453,18 @@ def test_full_size_union_of_seed_sets_is_elementwise_min(ctx, which):
     expect = torch.minimum(da, db)
     assert torch.equal(du, expect), int((du != expect).sum())
     assert ctx.stats()["device_error"] == 0
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.5, 1.0])
+def test_ref_union_of_seed_sets_is_elementwise_min_full_size(ctx, lam):
+    """ref-mode at the reference benchmark's image size (3648 x 2432 gray): T(A | B) == min(T(A), T(B))."""
+    rng = np.random.default_rng(29)
+    h, w = 2432, 3648
+    img = cuda(wl.blobs_gray(31, w, h))
+    a = cuda(wl.random_disks(rng, w, h, 8, 2, 6))
+    b = cuda(wl.random_disks(rng, w, h, 5, 2, 6))
+    da = dtb.generalised_distance_transform(img, a, lam, ctx=ctx)
+    db = dtb.generalised_distance_transform(img, b, lam, ctx=ctx)
+    du = dtb.generalised_distance_transform(img, a | b, lam, ctx=ctx)
+    expect = torch.minimum(da, db)
+    assert torch.equal(du, expect), int((du != expect).sum())

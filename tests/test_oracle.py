@@ -113,3 +113,15 @@ def test_ns_union_of_seed_sets_is_elementwise_min(rgb):
     for g in (0.02, 1.0):
         expect = np.minimum(orc.ggdt_ns(img, a, g), orc.ggdt_ns(img, b, g))
         assert_images_eq(orc.ggdt_ns(img, a | b, g), expect, "union, gamma %g" % g)
+
+
+@pytest.mark.parametrize("lam", [0.0, 0.5, 1.0])
+def test_ref_union_of_seed_sets_is_elementwise_min(lam):
+    from distance_transform_benchmarks_b200 import workloads as wl
+    rng = np.random.default_rng(6)
+    img = wl.blobs_gray(4, 140, 110)
+    a = wl.random_disks(rng, 140, 110, 3, 1, 4)
+    b = wl.random_disks(rng, 140, 110, 4, 1, 4)
+    for fma in (True, False):
+        expect = np.minimum(orc.ggdt_ref(img, a, lam, fma=fma), orc.ggdt_ref(img, b, lam, fma=fma))
+        assert_images_eq(orc.ggdt_ref(img, a | b, lam, fma=fma), expect, "ref union, fma %s" % fma)
