@@ -199,6 +199,8 @@ struct RepitchItem {
   uint32_t dst_pitch;
   uint32_t row_base;  // prefix of rows over the items of the launch
 };
+// Failure self-test: counts one queued tile that is never pushed (the run ends on its no-progress limit).
+__global__ void ggdt_phantom_pending(QueueHdr* hdr);
 __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restrict__ items, int n, uint32_t total_rows);
 Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns = DEFAULT_TIMEOUT_NS);
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.

@@ -445,7 +445,14 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(sc + L.o_tmap);
   const uint32_t* dbase = reinterpret_cast<const uint32_t*>(sc + L.o_base);
   uint32_t* states = reinterpret_cast<uint32_t*>(sc + L.o_states);
-  Queue q = make_queue(sc, L);
+  // dtb_debug_inject_queue_stall on the server's context applies to the next wave with tiles (one-shot).
+  uint64_t stall_ns = 0;
+  if (total > 0) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    stall_ns = ctx->inject_stall_ns;
+    ctx->inject_stall_ns = 0;
+  }
+  Queue q = make_queue(sc, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS);
   f.hdr = total > 0 ? reinterpret_cast<QueueHdr*>(sc + L.o_hdr) : nullptr;
   f.total = total;
   if (!items.empty()) {
@@ -465,6 +472,10 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
     if (!disks.empty()) {
       serve_seed_tiles<<<std::min<int>((int)disks.size(), 4096), 32, 0, st>>>(
           ddesc, reinterpret_cast<const DiskItem*>(sc + o_disks), (int)disks.size(), states, q);
+      DTB_CUDA(ctx, cudaGetLastError());
+    }
+    if (stall_ns) {
+      ggdt_phantom_pending<<<1, 1, 0, st>>>(q.hdr);
       DTB_CUDA(ctx, cudaGetLastError());
     }
     cudaLaunchConfig_t cfg{};

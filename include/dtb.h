@@ -208,9 +208,10 @@ DTB_API dtb_status dtb_gdt_noalloc(const dtb_image* img, const dtb_image* mask, 
                                    float v, void* stream);
 
 /* Failure-detection self-test (host-side injection, no device fault): the next persistent tile run of this
- * context counts one queued tile that is never pushed and uses timeout_ms (1..60000) as the no-progress limit
- * of its tile queue.  Its workers find no work, the bounded wait in every worker ends, the kernel returns and
- * the call reports DTB_ERR_TIMEOUT; the context stays usable for the next call.  One-shot. */
+ * context (a call, or the next wave of a server created on it) counts one queued tile that is never pushed and
+ * uses timeout_ms (1..60000) as the no-progress limit of its tile queue.  Its workers find no work, the bounded
+ * wait in every worker ends, the kernel returns and the call (or every request of the wave) reports
+ * DTB_ERR_TIMEOUT; the context and the server stay usable.  One-shot. */
 DTB_API dtb_status dtb_debug_inject_queue_stall(dtb_context ctx, uint32_t timeout_ms);
 
 /* Pitched image storage, reference dt::image2d<T> allocation (dt/include/dt/image2d.hpp:36-50,

@@ -149,3 +149,42 @@ def test_overlapping_small_waves_keep_per_image_order():
     assert st["completed"] == len(outs) and st["failed"] == 0
     assert st["waves"] >= len(outs) // 2
     srv.close()
+
+
+def test_failed_wave_fails_its_requests_only():
+    """A wave whose tile queue stalls (host-side injection: one phantom queued tile, short no-progress limit;
+    no device fault) completes its requests with DTB_ERR_TIMEOUT and drops its new image; the engine keeps
+    serving, and requests before and after it are exact."""
+    rng = np.random.default_rng(9)
+    batch = _images(35, 3, smin=60, smax=200)
+    ctx = dtb.Context(0)
+    srv = dtb.Server(128 << 20, ctx=ctx)
+
+    def new_image(i):
+        img, mask, g = batch[i]
+        out = torch.empty(img.shape[:2], dtype=torch.float32)
+        rid = srv.submit_image(i, torch.from_numpy(img), torch.from_numpy(mask), g, out)
+        return _drain(srv, 1)[rid]["status"], out
+
+    status, out0 = new_image(0)
+    assert status == 0
+    assert_images_eq(out0, orc.ggdt_ns(*batch[0]), "before the stall")
+    ctx.inject_queue_stall(100)
+    status, _ = new_image(1)
+    assert status == 4  # DTB_ERR_TIMEOUT
+    out = torch.empty(batch[1][0].shape[:2], dtype=torch.float32)
+    rid = srv.submit_edit(1, [(5, 5, 3)], out)
+    assert _drain(srv, 1)[rid]["status"] == 1  # the failed image was not kept
+    status, out2 = new_image(2)
+    assert status == 0
+    assert_images_eq(out2, orc.ggdt_ns(*batch[2]), "after the stall")
+    img, mask, g = batch[0]
+    disks = _disks(rng, img, 2)
+    out = torch.empty(img.shape[:2], dtype=torch.float32)
+    rid = srv.submit_edit(0, disks, out)
+    assert _drain(srv, 1)[rid]["status"] == 0
+    assert_images_eq(out, orc.ggdt_ns(img, _mask_with(mask, disks), g), "edit after the stall")
+    st = srv.stats()
+    assert st["failed"] == 2
+    srv.close()
+    ctx.close()
