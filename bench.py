@@ -141,29 +141,54 @@ def profiled_traffic_bytes_per_px():
 # ---------------------------------------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------------------------------------
-def link_floor(h2d, d2h, e2e_ms):
-    """The host link's own time for one e2e step: h2d bytes in and d2h bytes out as one copy each way from and
-    to pinned memory, concurrently on two streams (CUDA events), and each direction alone.  The e2e step
-    cannot be shorter than the concurrent copy."""
+def link_floor(h2d, d2h, e2e_ms, nchunks):
+    """The host link's own time for one e2e step, copies only, pinned memory, CUDA events: the step's h2d bytes
+    in and d2h bytes out concurrently on two streams as one copy each way (copy_floor_ms), as `nchunks` copies
+    each way like the host-buffer pipeline (chunked_copy_floor_ms), and with chunk k's copy out waiting for
+    chunk k + 2's copy in, a stand-in for the tile runs between them (pipelined_copy_floor_ms); and each
+    direction alone."""
     hin = torch.empty(h2d, dtype=torch.uint8).pin_memory()
     hout = torch.empty(d2h, dtype=torch.uint8).pin_memory()
     din = torch.empty(h2d, dtype=torch.uint8, device="cuda")
     dout = torch.empty(d2h, dtype=torch.uint8, device="cuda")
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
 
-    def timed(do_in, do_out, reps=3):
+    n = max(1, nchunks)
+    ci = [(k * h2d // n, (k + 1) * h2d // n) for k in range(n)]
+    co = [(k * d2h // n, (k + 1) * d2h // n) for k in range(n)]
+
+    def timed(do_in, do_out, reps=3, chunks=1, lag=None):
         best = None
         for _ in range(reps):
             a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
             torch.cuda.synchronize()
             a.record(s_in)
             s_out.wait_event(a)
-            if do_in:
-                with torch.cuda.stream(s_in):
-                    din.copy_(hin, non_blocking=True)
-            if do_out:
-                with torch.cuda.stream(s_out):
-                    hout.copy_(dout, non_blocking=True)
+            if chunks == 1:
+                if do_in:
+                    with torch.cuda.stream(s_in):
+                        din.copy_(hin, non_blocking=True)
+                if do_out:
+                    with torch.cuda.stream(s_out):
+                        hout.copy_(dout, non_blocking=True)
+            elif lag is None:
+                for (x, y), (u, v) in zip(ci, co):
+                    with torch.cuda.stream(s_in):
+                        din[x:y].copy_(hin[x:y], non_blocking=True)
+                    with torch.cuda.stream(s_out):
+                        hout[u:v].copy_(dout[u:v], non_blocking=True)
+            else:
+                ev = []
+                for x, y in ci:
+                    with torch.cuda.stream(s_in):
+                        din[x:y].copy_(hin[x:y], non_blocking=True)
+                    e = torch.cuda.Event()
+                    e.record(s_in)
+                    ev.append(e)
+                for k, (u, v) in enumerate(co):
+                    s_out.wait_event(ev[min(k + lag, n - 1)])
+                    with torch.cuda.stream(s_out):
+                        hout[u:v].copy_(dout[u:v], non_blocking=True)
             b.record(s_out)
             s_in.wait_event(b)
             c.record(s_in)
@@ -173,11 +198,15 @@ def link_floor(h2d, d2h, e2e_ms):
         return best
 
     both = timed(True, True)
+    chunked = timed(True, True, chunks=n)
+    lagged = timed(True, True, chunks=n, lag=2)
     t_in = timed(True, False)
     t_out = timed(False, True)
-    return {"copy_floor_ms": both, "frac": both / e2e_ms, "h2d_alone_gbs": h2d / t_in / 1e6,
-            "d2h_alone_gbs": d2h / t_out / 1e6, "e2e_d2h_gbs": d2h / e2e_ms / 1e6,
-            "note": "copy_floor_ms: the step's bytes in and out copied concurrently, pinned, one copy per direction"}
+    return {"copy_floor_ms": both, "frac": both / e2e_ms, "chunks": n, "chunked_copy_floor_ms": chunked,
+            "pipelined_copy_floor_ms": lagged, "frac_of_pipelined": lagged / e2e_ms,
+            "h2d_alone_gbs": h2d / t_in / 1e6, "d2h_alone_gbs": d2h / t_out / 1e6, "e2e_d2h_gbs": d2h / e2e_ms / 1e6,
+            "note": "copies only, pinned, concurrent in/out: one copy per direction; the pipeline's chunk count; "
+                    "and chunk k out after chunk k+2 in"}
 
 
 def cpu_baseline(batch, seconds):
@@ -531,7 +560,7 @@ def run_ours(args, dist):
         e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
         e2e["calls"] = "asynchronous, the last one synchronous (the timed region ends with the last copy out)"
         if dist.world == 1:
-            e2e["link"] = link_floor(h2d, d2h, ems)
+            e2e["link"] = link_floor(h2d, d2h, ems, int(ctx.stats()["rounds"]) // max(1, args.steps))
     if e2e is not None and dist.world == 1:
         # The same batch from separate pinned buffers per image (one copy per plane and direction).
         simgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]
