@@ -529,7 +529,6 @@ void retire_wave(dtb_server s, InFlight& f, dtb_status status) {
 void worker_main(dtb_server s) {
   cudaSetDevice(s->ctx->device);
   std::deque<InFlight> inflight;
-  int next_slot = 0;
   int64_t blocked_at = -1;  // submissions counted when an admission found nothing to run beside a wave in flight
   auto set_busy_from = [&] { s->busy_from = inflight.empty() ? s->wave_no + 1 : inflight.front().no; };
   for (;;) {
@@ -558,8 +557,7 @@ void worker_main(dtb_server s) {
       }
     }
     if (!f.reqs.empty()) {
-      f.slot = next_slot;
-      next_slot ^= 1;
+      f.slot = inflight.empty() ? 0 : (inflight.front().slot ^ 1);  // at most one wave is in flight here
       const dtb_status ls = launch_wave(s, f);
       if (ls != DTB_OK) {
         // Nothing of this wave may still run when its requests complete.
