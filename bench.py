@@ -559,8 +559,12 @@ def run_ours(args, dist):
         e2e["matches_device_run"] = bool(ok)
         e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
         e2e["calls"] = "asynchronous, the last one synchronous (the timed region ends with the last copy out)"
+        est = ctx.stats()  # the K timed calls (the last, synchronous one reports them all)
+        e2e["library_bytes_per_step"] = {"h2d": est["h2d_bytes"] // max(1, args.steps),
+                                         "d2h": est["d2h_bytes"] // max(1, args.steps),
+                                         "note": "bytes the host pipeline copied (h2d includes its descriptor tables)"}
         if dist.world == 1:
-            e2e["link"] = link_floor(h2d, d2h, ems, int(ctx.stats()["rounds"]) // max(1, args.steps))
+            e2e["link"] = link_floor(h2d, d2h, ems, int(est["rounds"]) // max(1, args.steps))
     if e2e is not None and dist.world == 1:
         # The same batch from separate pinned buffers per image (one copy per plane and direction).
         simgs = [torch.from_numpy(i).pin_memory() for i, _, _ in batch]

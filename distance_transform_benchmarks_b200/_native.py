@@ -58,6 +58,8 @@ class DtbStats(ctypes.Structure):
         ("device_error", ctypes.c_uint32),
         ("device_error_info", ctypes.c_uint32),
         ("kernel_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
     ]
 
 

@@ -270,16 +270,21 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
               reinterpret_cast<const uint8_t*>(items[k].data() + items[k].size()), host + h_items[k]);
     DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_chunk[k] + L[k].o_desc, host + h_tab[k], tab.size(), cudaMemcpyHostToDevice,
                                   ctx->s_in));
-    if (!items[k].empty())
+    ctx->pipe_h2d += tab.size();
+    if (!items[k].empty()) {
       DTB_CUDA(ctx, cudaMemcpyAsync(scratch + o_items[k], host + h_items[k], sizeof(RepitchItem) * items[k].size(),
                                     cudaMemcpyHostToDevice, ctx->s_in));
+      ctx->pipe_h2d += sizeof(RepitchItem) * items[k].size();
+    }
   }
   DTB_CUDA(ctx, cudaEventRecord(ev_host, ctx->s_in));
 
   // ---- the pipeline: copies in, tile runs on the two lanes, copies out ----
   for (int k = 0; k < nchunks; ++k) {
-    for (const Copy& c : cin[k])
+    for (const Copy& c : cin[k]) {
       if ((s = issue(ctx, c, stage, true, ctx->s_in)) != DTB_OK) return s;
+      ctx->pipe_h2d += c.width * c.rows;
+    }
     cudaEvent_t e_in = event_at(ctx, 1 + 3 * k);
     if (!e_in) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
     DTB_CUDA(ctx, cudaEventRecord(e_in, ctx->s_in));
@@ -303,8 +308,10 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     if (!e_run) return fail(ctx, DTB_ERR_CUDA, "cudaEventCreate failed");
     DTB_CUDA(ctx, cudaEventRecord(e_run, lane));
     DTB_CUDA(ctx, cudaStreamWaitEvent(ctx->s_out, e_run, 0));
-    for (const Copy& c : cout[k])
+    for (const Copy& c : cout[k]) {
       if ((s = issue(ctx, c, stage, false, ctx->s_out)) != DTB_OK) return s;
+      ctx->pipe_d2h += c.width * c.rows;
+    }
   }
   // The call's end: its last copy out (each chunk's run, which folded its status into ctx->dpipe, came before
   // that chunk's copy out).  Only copies run on s_out, so the next calls are not held up by a kernel waiting
@@ -328,8 +335,10 @@ dtb_status finish_pipeline(dtb_context ctx) {
   const dtb_status s = read_device_status(ctx, ctx->dpipe, &st);
   st.tiles = ctx->pipe_tiles;
   st.rounds = ctx->pipe_chunks;
+  st.h2d_bytes = ctx->pipe_h2d;
+  st.d2h_bytes = ctx->pipe_d2h;
   ctx->stats = st;
-  ctx->pipe_tiles = ctx->pipe_chunks = 0;
+  ctx->pipe_tiles = ctx->pipe_chunks = ctx->pipe_h2d = ctx->pipe_d2h = 0;
   DTB_CUDA(ctx, cudaMemset(ctx->dpipe, 0, sizeof(QueueHdr)));
   return s;
 }

@@ -118,7 +118,7 @@ struct dtb_context_s {
   dtb::QueueHdr* dpipe = nullptr;
   cudaEvent_t ev_pipe_done = nullptr;
   bool pipe_pending = false;
-  uint64_t pipe_tiles = 0, pipe_chunks = 0;
+  uint64_t pipe_tiles = 0, pipe_chunks = 0, pipe_h2d = 0, pipe_d2h = 0;
   // Host-buffer pipeline: two sets of device staging + chunk scratch used by alternate calls, so that a call's
   // copies in overlap the previous call's copies out; set i is free once ev_pset_free[i] (its last call's end)
   // has completed.

@@ -75,6 +75,8 @@ typedef struct dtb_stats {
   uint32_t device_error;  /* 0, or the device error code */
   uint32_t device_error_info;
   double kernel_ms;       /* DTB_FLAG_TIMING: device time of the tile kernel(s) of the call, else 0 */
+  uint64_t h2d_bytes;     /* host-buffer batches: bytes copied host -> device (images, masks, tables), else 0 */
+  uint64_t d2h_bytes;     /* host-buffer batches: bytes copied device -> host (maps), else 0 */
 } dtb_stats;
 
 DTB_API int32_t dtb_abi_version(void);

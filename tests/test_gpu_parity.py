@@ -299,6 +299,22 @@ def test_host_pipeline_alternate_buffer_sets():
     c.close()
 
 
+def test_host_pipeline_reports_bytes_moved():
+    """dtb_stats of a host-buffer batch counts the bytes copied each way: images and masks (plus the descriptor
+    tables) in, maps out."""
+    c = dtb.Context(0)
+    c.set_tuning(host_chunk_kpx=256)
+    batch = wl.config3(seed=42, n=12, smin=40, smax=400)
+    imgs = [torch.from_numpy(i) for i, _, _ in batch]
+    masks = [torch.from_numpy(m) for _, m, _ in batch]
+    dists = dtb.geodesic_distance_transform_batch(imgs, masks, [g for _, _, g in batch], ctx=c)
+    st = c.stats()
+    planes_in = sum(i.numel() + m.numel() for i, m in zip(imgs, masks))
+    assert planes_in < st["h2d_bytes"] < planes_in + (1 << 20)
+    assert st["d2h_bytes"] == sum(d.numel() * 4 for d in dists)
+    c.close()
+
+
 def test_batch_host_buffers(ctx):
     batch = wl.config3(seed=12, n=6, smin=40, smax=200)
     dists = dtb.geodesic_distance_transform_batch([torch.from_numpy(i) for i, _, _ in batch],
