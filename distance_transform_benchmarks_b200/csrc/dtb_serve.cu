@@ -318,7 +318,8 @@ struct InFlight {
 };
 
 // Enqueues one wave: copies in and table upload on s_in, tile work on s_run, copies out on s_out; ev_done of
-// the slot marks its end.  Requests of the wave reference no image of another wave in flight (admit), so the
+// the slot marks its end.  The caller holds the context's lock, as every API call on the context does (the
+// helpers below record failures in the context's message).  Requests of the wave reference no image of another wave in flight (admit), so the
 // waves' device work only shares the arena's free space and the tile-run stream.
 dtb_status launch_wave(dtb_server s, InFlight& f) {
   dtb_context ctx = s->ctx;
@@ -445,10 +446,10 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(sc + L.o_tmap);
   const uint32_t* dbase = reinterpret_cast<const uint32_t*>(sc + L.o_base);
   uint32_t* states = reinterpret_cast<uint32_t*>(sc + L.o_states);
-  // dtb_debug_inject_queue_stall on the server's context applies to the next wave with tiles (one-shot).
+  // dtb_debug_inject_queue_stall on the server's context applies to the next wave with tiles (one-shot; the
+  // caller holds ctx->mu).
   uint64_t stall_ns = 0;
   if (total > 0) {
-    std::lock_guard<std::mutex> lk(ctx->mu);
     stall_ns = ctx->inject_stall_ns;
     ctx->inject_stall_ns = 0;
   }
@@ -558,7 +559,11 @@ void worker_main(dtb_server s) {
     }
     if (!f.reqs.empty()) {
       f.slot = inflight.empty() ? 0 : (inflight.front().slot ^ 1);  // at most one wave is in flight here
-      const dtb_status ls = launch_wave(s, f);
+      dtb_status ls;
+      {
+        std::lock_guard<std::mutex> ctx_lock(s->ctx->mu);
+        ls = launch_wave(s, f);
+      }
       if (ls != DTB_OK) {
         // Nothing of this wave may still run when its requests complete.
         cudaStreamSynchronize(s->s_in);
@@ -591,7 +596,10 @@ void worker_main(dtb_server s) {
     }
     dtb_status status = cudaEventSynchronize(ev) == cudaSuccess ? DTB_OK : DTB_ERR_CUDA;
     dtb_stats ds{};
-    if (status == DTB_OK && old.hdr) status = read_device_status(s->ctx, old.hdr, &ds);
+    if (status == DTB_OK && old.hdr) {
+      std::lock_guard<std::mutex> ctx_lock(s->ctx->mu);
+      status = read_device_status(s->ctx, old.hdr, &ds);
+    }
     std::lock_guard<std::mutex> lk(s->mu);
     s->st.tile_visits += ds.tile_visits;
     s->st.tiles += old.total;
