@@ -71,3 +71,35 @@ def test_host_library_exports():
     lib = ctypes.CDLL(_native.LIBHOST_PATH)
     for name in ["dtbg_blobs_gray", "dtbg_voronoi_rgb", "dtbg_maze_gray", "dtbg_draw_disks"]:
         assert hasattr(lib, name)
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every struct of include/dtb.h, compiled as C: size and member offsets equal the ctypes mirror's."""
+    import shutil
+    import subprocess
+    nat = _native
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    structs = {"dtb_image": nat.DtbImage, "dtb_stats": nat.DtbStats, "dtb_tuning": nat.DtbTuning,
+               "dtb_serve_config": nat.DtbServeConfig, "dtb_serve_request": nat.DtbServeRequest,
+               "dtb_serve_completion": nat.DtbServeCompletion, "dtb_serve_stats": nat.DtbServeStats}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "dtb.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append('  printf("%s size %%zu\\n", sizeof(%s));' % (cname, cname))
+        for field, _ in py._fields_:
+            lines.append('  printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, field, cname, field))
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([cc, "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, what, val = line.split()
+        got[(cname, what)] = int(val)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
