@@ -30,8 +30,10 @@ sys.path.insert(0, ROOT)
 METRIC = "converged GGDT Mpixel/s, batched vs per-image on one B200; serve p50/p99 ms"
 UNIT = "Mpixel/s"
 PLAIN_SUBSET = 64          # images of the batch timed through the plain per-image path
-CPU_SAMPLE_SECONDS = 15.0  # bounded CPU baseline sample
-REF_STEP_MPX = 24.0        # reference arm: pixels per step
+REF_STEP_MPX = 24.0        # CPU legs (reference arm, cpu_baseline): pixels of the stratified sample per step
+PARITY_LARGE = 16          # oracle parity sample: images of the batch with a side >= 1536 ...
+PARITY_SPREAD = 16         # ... plus images at evenly spaced size quantiles
+FP64_TOL = 1e-5            # stated bound on the relative error against the FP64 Dijkstra
 
 
 def parse():
@@ -209,25 +211,54 @@ def link_floor(h2d, d2h, e2e_ms, nchunks):
                     "and chunk k out after chunk k+2 in"}
 
 
-def cpu_baseline(batch, seconds):
-    """The oracle (CPU restatement of the reference raster algorithm) on the host cores, over the batch's
-    images in order until `seconds` of work: Mpixel/s."""
+def bench_config(args, specs):
+    """The `config` object of the JSON line: the same dict in both arms (the workload, not how an arm samples
+    it)."""
+    return {"workload": "ragged batch of %d images per GPU, sides log-U[64,2048], half gray blobs / half rgb8 "
+                        "Voronoi, 1-8 seed disks r 2-6, gamma in {0.01,0.1,1.0}, seed %d" % (args.images, args.seed),
+            "pixels_per_gpu": int(sum(s[1] * s[2] for s in specs)), "parallelism": "replicas (independent images "
+            "per rank)", "l2": "inputs larger than L2 (no flush needed)"}
+
+
+def sample_desc(idx, specs):
+    px = sum(specs[i][1] * specs[i][2] for i in idx)
+    stride = idx[1] - idx[0] if len(idx) > 1 else 1
+    return "every %d-th image of the batch (%d images, %.1f Mpx, gray and rgb8 alternating)" % (stride, len(idx),
+                                                                                                  px / 1e6), px
+
+
+def parity_indices(specs):
+    """The oracle parity sample: the first PARITY_LARGE images with a side >= 1536 and PARITY_SPREAD images at
+    evenly spaced quantiles of the pixel count."""
+    large = [i for i, s in enumerate(specs) if max(s[1], s[2]) >= 1536][:PARITY_LARGE]
+    order = sorted(range(len(specs)), key=lambda i: specs[i][1] * specs[i][2])
+    spread = [order[int(round(q * (len(order) - 1) / max(1, PARITY_SPREAD - 1)))] for q in range(PARITY_SPREAD)]
+    return sorted(set(large) | set(spread))
+
+
+def cpu_legs(batch, specs, sample_idx, maps, config_maps):
+    """The CPU legs, rank 0 of a one-GPU run: the oracle (CPU restatement of the reference raster algorithm) on
+    the host cores, timed on the reference arm's stratified sample; the same oracle as the bit-exact checker of
+    the GPU maps of that sample and of the parity sample; and the FP64 Dijkstra as the accuracy bound per
+    configuration.  `maps[i]`: the GPU map of batch image i (host numpy); `config_maps`: name -> (img, mask,
+    gamma, GPU map) of the single-image configurations.  Returns (cpu_baseline, parity)."""
     from oracle import oracle as orc
-    px, t0 = 0, time.perf_counter()
-    n = 0
-    for img, mask, g in batch:
-        orc.ggdt_ns(img, mask, g)
-        px += img.shape[0] * img.shape[1]
-        n += 1
-        if time.perf_counter() - t0 > seconds:
-            break
-    dt = time.perf_counter() - t0
-    out = {"value": px / dt / 1e6, "unit": UNIT, "cores": orc.max_threads(), "kind": "port",
-           "sample": "first %d images of the batch (%.1f Mpx), %.1f s" % (n, px / 1e6, dt)}
+    desc, px = sample_desc(sample_idx, specs)
+    mism = {}
+    t_oracle = 0.0
+    for i in sample_idx:
+        img, mask, g = batch[i]
+        t0 = time.perf_counter()
+        ref = orc.ggdt_ns(img, mask, g)
+        t_oracle += time.perf_counter() - t0
+        mism[i] = int(np.count_nonzero(ref.view(np.uint32) != maps[i].view(np.uint32)))
+    out = {"value": px / t_oracle / 1e6, "unit": UNIT, "cores": orc.max_threads(), "kind": "port",
+           "sample": desc + ", %.1f s" % t_oracle}
+    sample = [batch[i] for i in sample_idx]
 
     def rate(fn, seconds):
         px, t0 = 0, time.perf_counter()
-        for img, mask, g in batch:
+        for img, mask, g in sample:
             fn(img, mask, g)
             px += img.shape[0] * img.shape[1]
             if time.perf_counter() - t0 > seconds:
@@ -238,15 +269,38 @@ def cpu_baseline(batch, seconds):
     # (one thread), and the reference weight (C8, lambda 0.5; the raster restatement is single-threaded).
     out["single_thread_mpx_s"] = rate(lambda i, m, g: orc.ggdt_ns(i, m, g, nthreads=1), 3.0)
     out["dijkstra_f64_mpx_s"] = rate(lambda i, m, g: orc.dijkstra_ns_f64(i, m, g), 3.0)
-    gray = [(i, m, g) for i, m, g in batch if i.ndim == 2]
-    px, t0 = 0, time.perf_counter()
+    gray = [(i, m, g) for i, m, g in sample if i.ndim == 2]
+    px_r, t0 = 0, time.perf_counter()
     for img, mask, _ in gray:
         orc.ggdt_ref(img, mask, 0.5)
-        px += img.size
+        px_r += img.size
         if time.perf_counter() - t0 > 3.0:
             break
-    out["ref_mode_lambda05_single_thread_mpx_s"] = px / (time.perf_counter() - t0) / 1e6
-    return out
+    out["ref_mode_lambda05_single_thread_mpx_s"] = px_r / (time.perf_counter() - t0) / 1e6
+
+    # Parity: the oracle sample (large and size-spread images) beside the stratified one.
+    extra = [i for i in parity_indices(specs) if i not in mism]
+    for i in extra:
+        img, mask, g = batch[i]
+        mism[i] = int(np.count_nonzero(orc.ggdt_ns(img, mask, g).view(np.uint32) != maps[i].view(np.uint32)))
+    checked = sorted(mism)
+
+    def rel64(img, mask, g, d32):
+        d64 = orc.dijkstra_ns_f64(img, mask, g)
+        sel = d64 > 0
+        return float((np.abs(d32[sel].astype(np.float64) - d64[sel]) / d64[sel]).max()) if sel.any() else 0.0
+
+    fp64 = {name: rel64(*cm) for name, cm in config_maps.items()}
+    fp64["C3_first64"] = max(rel64(*batch[i], maps[i]) for i in range(min(64, len(batch))))
+    parity = {"oracle_images": len(checked),
+              "oracle_images_side_ge_1536": sum(1 for i in checked if max(specs[i][1], specs[i][2]) >= 1536),
+              "oracle_pixels": int(sum(specs[i][1] * specs[i][2] for i in checked)),
+              "oracle_mismatches": int(sum(mism.values())),
+              "oracle_sample": "the cpu_baseline sample, the first %d images with a side >= 1536 and %d images at "
+                               "evenly spaced size quantiles; bit-exact comparison" % (PARITY_LARGE, PARITY_SPREAD),
+              "fp64_max_rel": fp64, "fp64_tol": FP64_TOL,
+              "fp64_within_tol": all(v < FP64_TOL for v in fp64.values())}
+    return out, parity
 
 
 SERVE_POOL = 48                 # distinct synthetic images behind the new-image requests
@@ -296,10 +350,11 @@ def run_ref_mode(args, ctx, stream):
 def run_configs(ctx, stream):
     """The single-image configurations, inputs resident on the device, one call each (3 timed): C0 (512^2 gray
     blobs), C1 (4096^2 gray maze: the worst case for raster passes, paths wind through the whole image) and C2
-    (8192^2 rgb8 Voronoi), with the tile visits and sweep phases behind each figure."""
+    (8192^2 rgb8 Voronoi), with the tile visits and sweep phases behind each figure.  Returns the figures and,
+    per configuration, (img, mask, gamma, map) for the FP64 error of the CPU legs."""
     import distance_transform_benchmarks_b200 as dtb
     from distance_transform_benchmarks_b200 import workloads as wl
-    out = {}
+    out, maps = {}, {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for name, gen in (("C0", wl.config0), ("C1", wl.config1), ("C2", wl.config2)):
         img, mask, gamma = gen()
@@ -318,7 +373,9 @@ def run_configs(ctx, stream):
                      "visits_per_tile": st["tile_visits"] / max(1, st["tiles"]),
                      "phases_per_visit": st["phases"] / max(1, st["tile_visits"]),
                      "activations_per_tile": st["activations"] / max(1, st["tiles"])}
-    return out
+        maps[name] = (img, mask, gamma, d.cpu().numpy())
+        del ti, tm, d
+    return out, maps
 
 
 def run_serve(args, dev):
@@ -412,17 +469,19 @@ def run_serve(args, dev):
 
 
 def run_reference(args, dist):
+    """The reference arm: the oracle (the reference's raster algorithm restated on the CPU; the reference itself
+    has no CPU implementation of the path) on all host cores, each step one pass over the stratified sample of
+    the batch.  The inputs come from the oracle's build of the workload generators, so this process loads only
+    libraries under oracle/."""
     if dist.rank != 0:
         return
     from distance_transform_benchmarks_b200 import workloads as wl
     from oracle import oracle as orc
+    wl.use_generator(orc.workload_generator_path())
     specs = wl.config3_specs(seed=args.seed, n=args.images)
-    sample, px = [], 0
-    for s in specs:
-        sample.append(wl.make_image(s))
-        px += s[1] * s[2]
-        if px >= args.ref_mpx * 1e6:
-            break
+    idx = wl.stratified_indices(specs, args.ref_mpx)
+    desc, px = sample_desc(idx, specs)
+    sample = [wl.make_image(specs[i]) for i in idx]
     for _ in range(args.warmup):
         for img, mask, g in sample[:4]:
             orc.ggdt_ns(img, mask, g)
@@ -434,12 +493,11 @@ def run_reference(args, dist):
         times.append(time.perf_counter() - t0)
     ms = 1e3 * statistics.mean(times)
     value = px / 1e6 / (ms / 1e3)
-    desc = "first %d images of the 1024-image batch (%.1f Mpx) per step" % (len(sample), px / 1e6)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "ragged batch of 1024 images (sides log-U[64,2048], gray blobs / rgb8 Voronoi)",
-                       "sample": desc},
+            "config": bench_config(args, specs),
+            "sample": desc,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": orc.max_threads(), "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -448,13 +506,15 @@ def run_reference(args, dist):
 def run_ours(args, dist):
     import distance_transform_benchmarks_b200 as dtb
     from distance_transform_benchmarks_b200 import workloads as wl
+    from distance_transform_benchmarks_b200.verify import ns_fixpoint_violations
 
     dev = dist.local
     torch.cuda.set_device(dev)
     ctx = dtb.Context(dev)
     stream = torch.cuda.current_stream()
 
-    batch = wl.config3(seed=dist.seed(args.seed), n=args.images)
+    specs = wl.config3_specs(seed=dist.seed(args.seed), n=args.images)
+    batch = [wl.make_image(sp) for sp in specs]
     px = wl.pixels(batch)
     alg_bytes = sum(img.shape[0] * img.shape[1] * wl.bytes_per_pixel(img) for img, _, _ in batch)
     imgs = [dtb.pitched_from(i) for i, _, _ in batch]
@@ -488,6 +548,34 @@ def run_ours(args, dist):
     px_all = dist.sum(px, "cuda")
     value = px_all / 1e6 / (ms_max / 1e3)
 
+    # Parity of the timed workload itself: every map of the last timed step satisfies the exact fixpoint
+    # characterisation (no edge can lower a value, every value is realised); the oracle compares a sample bit for
+    # bit in the CPU legs below.
+    viol = 0
+    for k in range(len(batch)):
+        va, vb, _ = ns_fixpoint_violations(imgs[k], masks[k], gammas[k], dtb.DEFAULT_V, dists[k])
+        viol += va + vb
+    maps = [d.cpu().numpy() for d in dists]
+
+    # The reference arm's stratified sample through the same path (plan, graph launch, device-resident), so the
+    # two arms can also be compared on identical pixels.
+    ref_idx = wl.stratified_indices(specs, args.ref_mpx)
+    ref_desc, ref_px = sample_desc(ref_idx, specs)
+    sub_plan = dtb.BatchPlan([imgs[i] for i in ref_idx], [masks[i] for i in ref_idx], [gammas[i] for i in ref_idx],
+                             dists=[dists[i] for i in ref_idx], ctx=ctx)
+    for _ in range(3):
+        sub_plan.run(stream)
+    sub_plan.wait(stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        sub_plan.run(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sub_plan.wait(stream)
+    ref_sample_ours = ref_px / 1e6 / (e0.elapsed_time(e1) / args.steps / 1e3)
+    sub_plan.close()
+
     # The same batch through the one-shot call (descriptors and tensor maps rebuilt per call, no graph; the
     # context reuses the autotuned launch).  Its DTB_FLAG_TIMING events, recorded on the launching stream
     # around the tile kernel, give the kernel's device time for the roofline.
@@ -503,27 +591,33 @@ def run_ours(args, dist):
     torch.cuda.synchronize()
     one_shot = px / 1e6 / (e0.elapsed_time(e1) / len(kernel_ms) / 1e3)
 
-    # Plain per-image path (host-driven rounds, one image per call) and persistent per-image calls.
-    sub = slice(0, min(PLAIN_SUBSET, len(batch)))
-    px_sub = sum(i.shape[0] * i.shape[1] for i, _, _ in batch[sub])
-    for _ in range(2):
-        dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx,
-                                              stream=stream, rounds=True)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx, stream=stream,
-                                          rounds=True)
-    torch.cuda.synchronize()
-    plain = px_sub / 1e6 / (time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    for k in range(sub.stop):
-        dtb.geodesic_distance_transform(imgs[k], masks[k], gammas[k], dist=dists[k], ctx=ctx, stream=stream)
-    torch.cuda.synchronize()
-    per_image_persistent = px_sub / 1e6 / (time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    dtb.geodesic_distance_transform_batch(imgs[sub], masks[sub], gammas[sub], dists=dists[sub], ctx=ctx, stream=stream)
-    torch.cuda.synchronize()
-    batched_sub = px_sub / 1e6 / (time.perf_counter() - t0)
+    # The per-image forms on the first PLAIN_SUBSET images: the plain path (host-driven rounds, one call per
+    # image, the structure of the reference's blocks variant), the persistent kernel called once per image, and
+    # the same images as one batched call.
+    sub = list(range(min(PLAIN_SUBSET, len(batch))))
+    px_sub = sum(batch[k][0].shape[0] * batch[k][0].shape[1] for k in sub)
+
+    def per_image(rounds):
+        for k in sub:
+            dtb.geodesic_distance_transform(imgs[k], masks[k], gammas[k], dist=dists[k], ctx=ctx, stream=stream,
+                                            rounds=rounds)
+
+    def batched():
+        dtb.geodesic_distance_transform_batch([imgs[k] for k in sub], [masks[k] for k in sub], [gammas[k] for k in sub],
+                                              dists=[dists[k] for k in sub], ctx=ctx, stream=stream)
+
+    rates = {}
+    for name, fn in (("plain", lambda: per_image(True)), ("persistent", lambda: per_image(False)), ("batched", batched)):
+        fn()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            best = t if best is None else min(best, t)
+        rates[name] = px_sub / 1e6 / best
 
     # End to end through the C ABI with pinned host buffers.
     e2e = None
@@ -555,8 +649,8 @@ def run_ours(args, dist):
         ems = dist.max(e0.elapsed_time(e1) / args.steps, "cuda")
         e2e = {"value": px_all / 1e6 / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": ems}
-        ok = all(torch.equal(hd, d.cpu()) for hd, d in zip(hdists[:8], dists[:8]))
-        e2e["matches_device_run"] = bool(ok)
+        e2e["maps_equal_device_run"] = bool(all(np.array_equal(hd.numpy().view(np.uint32), m.view(np.uint32))
+                                                for hd, m in zip(hdists, maps)))
         e2e["host_layout"] = "one pinned arena per plane kind (images, masks, distance maps)"
         e2e["calls"] = "asynchronous, the last one synchronous (the timed region ends with the last copy out)"
         est = ctx.stats()  # the K timed calls (the last, synchronous one reports them all)
@@ -590,15 +684,22 @@ def run_ours(args, dist):
                     "peak_kind": peak_kind, "kernel": "ggdt_persistent", "kernel_ms": kms,
                     "algorithmic_bytes": alg_bytes, "traffic": (bpp * px) if bpp else None}
 
-    cpu = None
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(batch, CPU_SAMPLE_SECONDS)
-    # The reference-shape and serving legs run in single-GPU runs only (with N ranks every rank would repeat
-    # them on its own GPU; the job's line reports the batch and e2e legs, reduced over ranks).
-    ref_mode = None if (args.no_ref_mode or dist.world > 1) else run_ref_mode(args, ctx, stream)
-    configs = None if (args.no_configs or dist.world > 1) else run_configs(ctx, stream)
+    # The reference-shape, single-image and serving legs run in single-GPU runs only (with N ranks every rank
+    # would repeat them on its own GPU; the job's line reports the batch and e2e legs, reduced over ranks).
+    one_gpu = dist.world == 1
+    ref_mode = None if (args.no_ref_mode or not one_gpu) else run_ref_mode(args, ctx, stream)
+    configs, config_maps = (None, {}) if (args.no_configs or not one_gpu) else run_configs(ctx, stream)
+    cpu = parity = None
+    if dist.rank == 0 and one_gpu and not args.no_cpu_baseline:
+        cpu, parity = cpu_legs(batch, specs, ref_idx, maps, config_maps)
+    config_maps = None
+    if parity is None:
+        parity = {}
+    parity.update({"fixpoint_images": len(batch), "fixpoint_violations": viol,
+                   "fixpoint_check": "every map of the timed batch: no edge lowers a value and every value is "
+                                     "realised (exact greatest-fixpoint characterisation, on the GPU)"})
     serve = None
-    if not args.no_serve and dist.world == 1:
+    if not args.no_serve and one_gpu:
         himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
         serve = run_serve(args, dev)
 
@@ -606,15 +707,22 @@ def run_ours(args, dist):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "ragged batch of %d images per GPU, sides log-U[64,2048], half gray blobs / half "
-                                       "rgb8 Voronoi, 1-8 seed disks r 2-6, gamma in {0.01,0.1,1.0}" % args.images,
-                           "pixels_per_gpu": px, "parallelism": "replicas (independent images per rank)",
-                           "l2": "inputs larger than L2 (no flush needed)",
-                           "launch": "one CUDA graph per step: queue reset, seed scan, persistent tile kernel, finalize"},
-                "per_image": {"plain_rounds_mpx_s": plain, "persistent_per_image_mpx_s": per_image_persistent,
-                              "batched_same_subset_mpx_s": batched_sub, "subset_images": sub.stop,
-                              "batched_vs_plain": value / plain if plain else None,
-                              "batched_vs_persistent_per_image": value / per_image_persistent},
+                "config": bench_config(args, specs),
+                "launch": "one CUDA graph per step: queue reset, seed scan, persistent tile kernel, finalize",
+                "parity": parity,
+                "reference_sample": {"sample": ref_desc, "ours_mpx_s": ref_sample_ours,
+                                     "note": "the reference arm's per-step sample through the same graph-launched "
+                                             "plan, device-resident"},
+                "per_image": {"subset": "first %d images of the batch (%.1f Mpx)" % (len(sub), px_sub / 1e6),
+                              "plain_per_image_mpx_s": rates["plain"],
+                              "persistent_per_image_mpx_s": rates["persistent"],
+                              "batched_mpx_s": rates["batched"],
+                              "batched_vs_plain": rates["batched"] / rates["plain"],
+                              "batched_vs_persistent_per_image": rates["batched"] / rates["persistent"],
+                              "note": "plain = host-driven rounds (the reference's blocks-variant structure), one "
+                                      "call per image; persistent = one persistent-kernel call per image; batched = "
+                                      "the same images in one call; wall clock, best of 3"},
+                "full_batch_graph_vs_plain_per_image": value / rates["plain"],
                 "one_shot_call_mpx_s": one_shot, "autotuned": tuning,
                 "tile_stats": {"tiles": stats["tiles"], "visits_per_tile": stats["tile_visits"] / max(1, stats["tiles"]),
                                "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},

@@ -175,21 +175,25 @@ def lib():
     return _lib
 
 
+def declare_generator(H):
+    """Declares the argument types of the generator entry points (csrc/datagen.cpp) on a loaded library."""
+    P, I, I64, U64, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
+    H.dtbg_blobs_gray.restype = None
+    H.dtbg_blobs_gray.argtypes = [U64, I, I, I, D, D, D, D, D, P, I64]
+    H.dtbg_voronoi_rgb.restype = None
+    H.dtbg_voronoi_rgb.argtypes = [U64, I, I, I, D, P, I64]
+    H.dtbg_maze_gray.restype = I
+    H.dtbg_maze_gray.argtypes = [U64, I, I, I, I, I, P, I64, ctypes.POINTER(I), ctypes.POINTER(I)]
+    H.dtbg_draw_disks.restype = None
+    H.dtbg_draw_disks.argtypes = [P, I64, I, I, I, P, P, P]
+    return H
+
+
 def host():
     """The host-only generator library."""
     global _host
     if _host is None:
         if not os.path.exists(LIBHOST_PATH):
             raise RuntimeError("libdtb_host.so is missing at %s: build it with __graft_entry__.build()" % LIBHOST_PATH)
-        H = ctypes.CDLL(LIBHOST_PATH)
-        P, I, I64, U64, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double
-        H.dtbg_blobs_gray.restype = None
-        H.dtbg_blobs_gray.argtypes = [U64, I, I, I, D, D, D, D, D, P, I64]
-        H.dtbg_voronoi_rgb.restype = None
-        H.dtbg_voronoi_rgb.argtypes = [U64, I, I, I, D, P, I64]
-        H.dtbg_maze_gray.restype = I
-        H.dtbg_maze_gray.argtypes = [U64, I, I, I, I, I, P, I64, ctypes.POINTER(I), ctypes.POINTER(I)]
-        H.dtbg_draw_disks.restype = None
-        H.dtbg_draw_disks.argtypes = [P, I64, I, I, I, P, P, P]
-        _host = H
+        _host = declare_generator(ctypes.CDLL(LIBHOST_PATH))
     return _host

@@ -348,7 +348,7 @@ __device__ __forceinline__ float ns_weight(uint32_t pa, uint32_t pb, float g2) {
   return ns_weight_sq(__dp4a(ad, ad, 0u), g2);
 }
 
-// ref-mode relaxation of one edge, reference dt/src/dt_block_passes.cuh:252-253:
+// ref-mode relaxation of one edge, reference dt/src/dt_block_passes.cuh:45-46:
 //   D(q) + l_eucl * local_dist2d[k] + l_grad * |I(p) - I(q)|
 template <bool FMA>
 __device__ __forceinline__ float ref_relax(float dq, float eucl_d, float l_eucl, float l_grad, float absdi) {

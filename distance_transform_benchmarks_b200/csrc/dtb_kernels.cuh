@@ -141,8 +141,10 @@ __device__ __forceinline__ float* dist_row(const ImgDesc& dd, int y) {
 // line an SM cached earlier can be returned.
 __device__ __forceinline__ float ld_dist(const ImgDesc& dd, int y, int x) { return __ldcg(dist_row(dd, y) + x); }
 
-// Waits for the TMA transactions of this warp's slot.  Bounded: on timeout the error word is set and the
-// wait goes on (bounded again) so that no copy is left in flight when the warp leaves.
+// Waits for the TMA transactions of this warp's slot.  Bounded: after TMA_TIMEOUT_NS the error word is set
+// and the wait goes on for as long again, to give a slow copy the chance to land before the warp leaves; after
+// that the wait gives up, and a copy may then still be pending.  The error word ends the launch: every later
+// pop returns POP_NONE, so the warp issues no further copy and never waits on this barrier again.
 __device__ __forceinline__ bool tma_wait(WarpSmem& sm, uint32_t& parity, const Queue& q, uint32_t tile) {
   const uint64_t t0 = globaltimer();
   bool ok = true;

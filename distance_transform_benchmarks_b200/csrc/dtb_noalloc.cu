@@ -38,8 +38,7 @@ constexpr size_t na_align(size_t x) { return (x + 255) / 256 * 256; }
 constexpr size_t OFF_HDR = 0;
 constexpr size_t OFF_DESC = na_align(OFF_HDR + sizeof(QueueHdr));
 constexpr size_t OFF_TMAP = na_align(OFF_DESC + sizeof(ImgDesc));
-constexpr size_t OFF_BASE = na_align(OFF_TMAP + 2 * sizeof(CUtensorMap));
-constexpr size_t OFF_STATES = na_align(OFF_BASE + 2 * sizeof(uint32_t));
+constexpr size_t OFF_STATES = na_align(OFF_TMAP + 2 * sizeof(CUtensorMap));
 constexpr size_t OFF_RING = na_align(OFF_STATES + 4ull * NOALLOC_MAX_TILES);
 constexpr size_t NOALLOC_BYTES = na_align(OFF_RING + 4ull * NOALLOC_RING);
 
@@ -123,9 +122,13 @@ __global__ void __launch_bounds__(128) noalloc_finalize(uint32_t tiles) {
   }
 }
 
-// Per-device set-up, done by the first call on each device with that device current.
+// Per-device set-up, done by the first call on each device with that device current, and again after the
+// device's context changed (cudaDeviceReset ends the primary context; the symbol address and the kernel
+// attribute belong to the old one).
+typedef CUresult (*PFN_ctx_get_current)(CUcontext*);
 struct NoallocDevice {
   bool ready = false;
+  CUcontext ctx = nullptr;     // context the entry below was set up in
   uint8_t* scratch = nullptr;  // device address of g_noalloc_scratch on this device
   int num_sms = 0;
   int blocks_per_sm = 0;
@@ -135,10 +138,25 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 NoallocDevice g_devices[NOALLOC_MAX_DEVICES];
 std::mutex g_setup_mu;
 
+PFN_ctx_get_current g_ctx_get_current = nullptr;
+
 dtb_status noalloc_setup(int dev, NoallocDevice** out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return DTB_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lk(g_setup_mu);
+  if (!g_ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &qr) != cudaSuccess ||
+        qr != cudaDriverEntryPointSuccess || !fn)
+      return DTB_ERR_NO_DEVICE;
+    g_ctx_get_current = reinterpret_cast<PFN_ctx_get_current>(fn);
+  }
+  // cudaSetDevice on the current device makes its primary context current (initialising it if needed).
+  if (cudaSetDevice(dev) != cudaSuccess) return DTB_ERR_CUDA;
+  CUcontext cur = nullptr;
+  if (g_ctx_get_current(&cur) != CUDA_SUCCESS || !cur) return DTB_ERR_NO_DEVICE;
   NoallocDevice& d = g_devices[dev];
+  if (d.ready && d.ctx != cur) d = NoallocDevice{};
   if (!d.ready) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DTB_ERR_CUDA;
@@ -158,6 +176,7 @@ dtb_status noalloc_setup(int dev, NoallocDevice** out) {
     d.num_sms = sms;
     d.blocks_per_sm = bps;
     d.encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    d.ctx = cur;
     d.ready = true;
   }
   *out = &d;
@@ -239,14 +258,12 @@ extern "C" DTB_API dtb_status dtb_gdt_noalloc(const dtb_image* img, const dtb_im
                       img->elem_size == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY, IMG_BOX_ROWS) ||
       !noalloc_encode(*nd, &tm[1], mask->buffer, (uint64_t)W, (uint64_t)H, (uint64_t)mask->pitch, TILE, TILE))
     return DTB_ERR_INVALID_ARG;
-  const uint32_t base[2] = {0u, tiles};
 
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   uint8_t* sc = nd->scratch;
   // Source buffers are pageable host memory: each copy has consumed its source when the call returns.
   if (cudaMemcpyAsync(sc + OFF_DESC, &desc, sizeof(desc), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(sc + OFF_TMAP, tm, sizeof(tm), cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemcpyAsync(sc + OFF_BASE, base, sizeof(base), cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemsetAsync(sc + OFF_HDR, 0, sizeof(QueueHdr), st) != cudaSuccess ||
       cudaMemsetAsync(sc + OFF_RING, 0, 4ull * NOALLOC_RING, st) != cudaSuccess)
     return DTB_ERR_CUDA;

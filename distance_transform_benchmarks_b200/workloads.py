@@ -12,14 +12,30 @@ these generators produce inputs with the configured shapes and value distributio
 * ``config3``: ragged batch of 1024 images, sides log-uniform in [64, 2048] (independent H and W), even index
   gray blobs / odd index rgb8 Voronoi, 1-8 seed disks of radius 2-6, gamma from {0.01, 0.1, 1.0}.
 
-Per-image parameters come from numpy's PCG64; pixels from the C++ generators of libdtb_host.so.
+Per-image parameters come from numpy's PCG64; pixels from the C++ generators of csrc/datagen.cpp, loaded from
+libdtb_host.so unless ``use_generator`` names another build of the same source (bench.py's CPU reference arm
+uses the oracle's copy, so that process loads no library of this package).
 """
 import ctypes
 import math
 
 import numpy as np
 
-from ._native import host
+from ._native import declare_generator, host
+
+_gen_lib = None
+
+
+def use_generator(path):
+    """Takes the pixel generators from the shared library at `path`, a build of csrc/datagen.cpp (same source,
+    same pixels), instead of libdtb_host.so."""
+    global _gen_lib
+    _gen_lib = declare_generator(ctypes.CDLL(path))
+
+
+def _gen():
+    return _gen_lib if _gen_lib is not None else host()
+
 
 GAMMA_C0 = np.float32(np.float32(1.0) / np.float32(255.0) * np.float32(10.0))
 
@@ -31,20 +47,20 @@ def _seed_of(*parts):
 
 def blobs_gray(seed, w, h, nblobs=16, smin=20.0, smax=80.0, amin=0.0, amax=255.0, noise=4.0):
     out = np.empty((h, w), np.uint8)
-    host().dtbg_blobs_gray(seed, w, h, nblobs, smin, smax, amin, amax, noise, out.ctypes.data, w)
+    _gen().dtbg_blobs_gray(seed, w, h, nblobs, smin, smax, amin, amax, noise, out.ctypes.data, w)
     return out
 
 
 def voronoi_rgb(seed, w, h, nsites=256, noise=6.0):
     out = np.empty((h, w, 3), np.uint8)
-    host().dtbg_voronoi_rgb(seed, w, h, nsites, noise, out.ctypes.data, 3 * w)
+    _gen().dtbg_voronoi_rgb(seed, w, h, nsites, noise, out.ctypes.data, 3 * w)
     return out
 
 
 def maze_gray(seed, w, h, cell=32, wall=4, noise_max=8):
     out = np.empty((h, w), np.uint8)
     sx, sy = ctypes.c_int(), ctypes.c_int()
-    r = host().dtbg_maze_gray(seed, w, h, cell, wall, noise_max, out.ctypes.data, w, ctypes.byref(sx), ctypes.byref(sy))
+    r = _gen().dtbg_maze_gray(seed, w, h, cell, wall, noise_max, out.ctypes.data, w, ctypes.byref(sx), ctypes.byref(sy))
     if r != 0:
         raise ValueError("bad maze parameters")
     return out, (sx.value, sy.value)
@@ -57,7 +73,7 @@ def disks_mask(w, h, centres, radii):
         cx = np.ascontiguousarray([c[0] for c in centres], np.int32)
         cy = np.ascontiguousarray([c[1] for c in centres], np.int32)
         r = np.ascontiguousarray(radii, np.int32)
-        host().dtbg_draw_disks(mask.ctypes.data, w, w, h, n, cx.ctypes.data, cy.ctypes.data, r.ctypes.data)
+        _gen().dtbg_draw_disks(mask.ctypes.data, w, w, h, n, cx.ctypes.data, cy.ctypes.data, r.ctypes.data)
     return mask
 
 
@@ -113,6 +129,16 @@ def make_image(spec):
 
 def config3(seed=3, n=1024, smin=64, smax=2048):
     return [make_image(s) for s in config3_specs(seed, n, smin, smax)]
+
+
+def stratified_indices(specs, target_mpx):
+    """Every k-th image of a batch (k odd, so gray and rgb8 images alternate in the sample), k chosen so that the
+    sample holds about `target_mpx` million pixels: a deterministic sample with the batch's size and kind mix."""
+    total = sum(s[1] * s[2] for s in specs)
+    k = max(1, int(round(total / max(1.0, target_mpx * 1e6))))
+    if k % 2 == 0:
+        k += 1
+    return list(range(0, len(specs), k))
 
 
 def pixels(batch):

@@ -8,7 +8,7 @@
  * Parity pinning
  *   ref-mode (C8, lambda blend, gray) is pinned by the two golden tensors of the reference test suite
  *   (tests/distance_transform.cpp:14-281 and :283-476), extracted by tests/golden/make_golden.py and
- *   checked bit-exactly in tests/test_oracle_golden.py.
+ *   checked bit-exactly in tests/test_oracle.py.
  *   ns-mode (C4, w = sqrt(1 + g2*dI^2), gray or rgb8) has no counterpart in the reference, so it is
  *   "parity unpinned" with respect to the reference: it shares the fixpoint solver with ref-mode and is
  *   cross-checked against the FP64 Dijkstra below.
@@ -23,7 +23,7 @@
  *   backward rows, forward columns, backward columns, repeated until nothing changes) is used here.
  *
  *   ref-mode relax, reference dt/src/generalised_distance_transform.cu:44-45 and
- *   dt/src/dt_block_passes.cuh:252-253:
+ *   dt/src/dt_block_passes.cuh:45-46:
  *        D(q) + l_eucl * local_dist2d[k] + l_grad * |I(p) - I(q)|
  *   with local_dist2d = {sqrt(2), 1, sqrt(2)} (generalised_distance_transform.cu:111), l_grad = lambda,
  *   l_eucl = 1 - lambda (:108-109), |I(p) - I(q)| on uint8 (dt/src/utils.cuh:38-41).  The reference is
@@ -67,7 +67,7 @@ static void init_map(const uint8_t* mask, int mask_pitch, float* D, int W, int H
 
 static inline float ref_relax(float dq, float eucl_term_d, float l_eucl, float l_grad, int absdi, int use_fma)
 {
-  /* reference dt/src/dt_block_passes.cuh:253: D[..] + l_eucl * local_dist2d[dy + 1] + l_grad * l_dist */
+  /* reference dt/src/dt_block_passes.cuh:46: D[..] + l_eucl * local_dist2d[dy + 1] + l_grad * l_dist */
   if (use_fma)
     return fmaf(l_grad, (float)absdi, fmaf(l_eucl, eucl_term_d, dq));
   float t = dq + l_eucl * eucl_term_d;

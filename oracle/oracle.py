@@ -13,16 +13,24 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
+WORKLOADS_PATH = os.path.join(HERE, "libworkloads.so")
 REF_PASSES_PATH = os.path.join(HERE, "_ref", "libref_passes.so")
 _lib = None
 _ref_lib = None
 
 
 def build(force=False):
-    src = os.path.join(HERE, "ggdt_oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(src) > os.path.getmtime(LIB_PATH):
-        subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []), check=True)
+    """Builds liboracle.so and libworkloads.so (make's own dependency check decides what is stale)."""
+    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []), check=True)
     return LIB_PATH
+
+
+def workload_generator_path():
+    """The oracle's build of the package's seeded workload generators (csrc/datagen.cpp): the same pixels as
+    libdtb_host.so, for processes that must not load a library of the package (bench.py's reference arm)."""
+    if not os.path.exists(WORKLOADS_PATH):
+        build()
+    return WORKLOADS_PATH
 
 
 REF_TESTS = ("image_view", "image2d", "c4", "rgb8", "io", "transfert", "distance_transform")

@@ -10,7 +10,8 @@ Reads tests/distance_transform.cpp of the reference project as text (it is never
 Both calls use the API default v = 1e10 (dt/include/dt/generalised_distance_transform.hpp:8,11).
 The float literals are converted the way the C++ compiler does: decimal -> double -> float.
 
-Usage: python tests/golden/make_golden.py [path/to/reference/tests/distance_transform.cpp]
+Usage: python tests/golden/make_golden.py path/to/reference/tests/distance_transform.cpp
+       (or set DTB_REFERENCE_ROOT to the reference project's root)
 """
 import os
 import re
@@ -19,7 +20,6 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/tests/distance_transform.cpp"
 
 
 def _strip_comments(text):
@@ -85,4 +85,9 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_SRC)
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("DTB_REFERENCE_ROOT"):
+        main(os.path.join(os.environ["DTB_REFERENCE_ROOT"], "tests", "distance_transform.cpp"))
+    else:
+        sys.exit("usage: make_golden.py <reference>/tests/distance_transform.cpp (or set DTB_REFERENCE_ROOT)")

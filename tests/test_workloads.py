@@ -52,3 +52,33 @@ def test_config3_specs():
     assert [k for k, *_ in specs[:4]] == ["gray", "rgb8", "gray", "rgb8"]
     mpx = sum(w * h for _, w, h, _, _ in specs) / 1e6
     assert 250 < mpx < 450  # E[area] = 572.5^2 -> ~335 Mpx
+
+
+def test_oracle_generator_build_gives_the_same_pixels():
+    """bench.py's CPU reference arm makes its inputs with the oracle's build of the generators (so it loads no
+    library of the package); both builds of csrc/datagen.cpp must give the same pixels."""
+    import os, subprocess, sys
+    code = ("import hashlib, sys; from distance_transform_benchmarks_b200 import workloads as wl\n"
+            "if sys.argv[1] == 'oracle':\n"
+            "    from oracle import oracle as orc; wl.use_generator(orc.workload_generator_path())\n"
+            "specs = wl.config3_specs(n=6, smax=300)\n"
+            "h = hashlib.md5()\n"
+            "for s in specs:\n"
+            "    img, mask, g = wl.make_image(s); h.update(img.tobytes()); h.update(mask.tobytes())\n"
+            "h.update(wl.maze_gray(5, 200, 160)[0].tobytes())\n"
+            "print(h.hexdigest())\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = [subprocess.run([sys.executable, "-c", code, which], capture_output=True, text=True, cwd=root, check=True)
+            .stdout for which in ("package", "oracle")]
+    assert outs[0] and outs[0] == outs[1]
+
+
+def test_stratified_sample_mixes_kinds_and_sizes():
+    specs = wl.config3_specs()
+    idx = wl.stratified_indices(specs, 24.0)
+    k = idx[1] - idx[0]
+    assert k % 2 == 1 and idx == list(range(0, len(specs), k))
+    kinds = {specs[i][0] for i in idx}
+    assert kinds == {"gray", "rgb8"}
+    mpx = sum(specs[i][1] * specs[i][2] for i in idx) / 1e6
+    assert 10 < mpx < 60
