@@ -440,6 +440,21 @@ def run_serve(args, dev):
     drain(lat, submitted, t0 + arrivals[-1] + 120)
     elapsed = time.perf_counter() - t0
     st = srv.stats()
+
+    def phases(a, b):
+        """Where the time of the waves between stats a and b went (per wave: host preparation, copies in, tile
+        run, copies out on their streams; per request: queueing before its wave's preparation)."""
+        w = max(1, b["waves"] - a["waves"])
+        r = max(1, b["completed"] - a["completed"])
+        return {"waves": int(b["waves"] - a["waves"]), "waves_split": int(b["waves_split"] - a["waves_split"]),
+                "host_prep_ms_per_wave": (b["host_prep_ms"] - a["host_prep_ms"]) / w,
+                "copy_in_ms_per_wave": (b["copy_in_ms"] - a["copy_in_ms"]) / w,
+                "kernel_ms_per_wave": (b["kernel_ms"] - a["kernel_ms"]) / w,
+                "copy_out_ms_per_wave": (b["copy_out_ms"] - a["copy_out_ms"]) / w,
+                "queue_wait_mean_ms": (b["queue_wait_ms"] - a["queue_wait_ms"]) / r,
+                "queue_wait_max_ms": b["queue_wait_max_ms"]}
+
+    zero = {k: 0 for k in st}
     # Saturated phase: the same mix submitted at once; throughput = the engine's capacity.
     ns = args.serve_saturated
     saturated = None
@@ -455,7 +470,7 @@ def run_serve(args, dev):
         saturated = {"requests": ns, "completed": len(lat2), "failed": int(st2["failed"] - st["failed"]),
                      "throughput_rps": len(lat2) / el2, "mpx_s": px2 / 1e6 / el2,
                      "waves": int(st2["waves"] - st["waves"]), "p50_ms": float(np.percentile(lat2, 50)),
-                     "p99_ms": float(np.percentile(lat2, 99)),
+                     "p99_ms": float(np.percentile(lat2, 99)), "phases": phases(st, st2),
                      "note": "all requests submitted at t=0 (latency includes queueing behind earlier requests)"}
     srv.close()
     lat = np.array(lat)
@@ -463,7 +478,7 @@ def run_serve(args, dev):
             "failed": int(st["failed"]), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "throughput_rps": len(lat) / elapsed, "mpx_s": px / 1e6 / elapsed,
             "waves": int(st["waves"]), "requests_per_wave": len(lat) / max(1, st["waves"]),
-            "hbm_budget_gb": SERVE_BUDGET / 2 ** 30, "evictions": int(st["evictions"]),
+            "hbm_budget_gb": SERVE_BUDGET / 2 ** 30, "evictions": int(st["evictions"]), "phases": phases(zero, st),
             "images": "sides log-U[256,4096], half gray blobs / half rgb8 Voronoi, %d distinct" % SERVE_POOL,
             "saturated": saturated}
 

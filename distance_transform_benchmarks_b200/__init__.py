@@ -54,13 +54,20 @@ class Context:
         self.check(lib().dtb_last_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in DtbStats._fields_}
 
-    def set_tuning(self, ctas_per_sm=0, grid_percent=0, host_chunk_kpx=0):
-        self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(DtbTuning(ctas_per_sm, grid_percent, host_chunk_kpx))))
+    def set_tuning(self, ctas_per_sm=0, grid_percent=0, host_chunk_kpx=0, queue_buckets=0, bucket_width_pct=0, staging=0):
+        """dtb_context_set_tuning: 0 keeps a field (see include/dtb.h for the ranges)."""
+        t = DtbTuning(ctas_per_sm, grid_percent, host_chunk_kpx, queue_buckets, bucket_width_pct, staging)
+        self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self):
         t = DtbTuning()
         self.check(lib().dtb_context_get_tuning(self._h, ctypes.byref(t)))
-        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent, "host_chunk_kpx": t.host_chunk_kpx}
+        return _tuning_dict(t)
+
+    def set_tuning_cache(self, path):
+        """dtb_context_set_tuning_cache: load this GPU's autotuner results from the JSON file at `path` and save
+        new ones there (None turns the cache off)."""
+        self.check(lib().dtb_context_set_tuning_cache(self._h, None if path is None else str(path).encode()))
 
     def sync(self, stream=None):
         self.check(lib().dtb_sync(self._h, ctypes.c_void_p(_stream_ptr(stream))))
@@ -80,6 +87,10 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def _tuning_dict(t):
+    return {f: getattr(t, f) for f, _ in DtbTuning._fields_}
 
 
 _ctx_lock = threading.Lock()
@@ -405,7 +416,12 @@ class BatchPlan:
             stream = torch.cuda.current_stream()
         t = DtbTuning()
         self.ctx.check(lib().dtb_plan_autotune(self._h, ctypes.c_void_p(_stream_ptr(stream)), int(reps), ctypes.byref(t)))
-        return {"ctas_per_sm": t.ctas_per_sm, "grid_percent": t.grid_percent}
+        return _tuning_dict(t)
+
+    def tuning(self):
+        t = DtbTuning()
+        self.ctx.check(lib().dtb_plan_get_tuning(self._h, ctypes.byref(t)))
+        return _tuning_dict(t)
 
     def close(self):
         if self._h:
@@ -424,9 +440,11 @@ class Server:
     output map are host tensors (pinned memory copies fastest); they are kept alive here until the request's
     completion has been polled."""
 
-    def __init__(self, hbm_budget_bytes, *, max_wave_requests=0, v=DEFAULT_V, ctx=None, device=0):
+    def __init__(self, hbm_budget_bytes, *, max_wave_requests=0, v=DEFAULT_V, max_wave_tiles=0, wave_stage_bytes=0,
+                 ctx=None, device=0):
         self.ctx = ctx if ctx is not None else default_context(device)
-        cfg = DtbServeConfig(int(hbm_budget_bytes), int(max_wave_requests), float(v))
+        cfg = DtbServeConfig(int(hbm_budget_bytes), int(max_wave_requests), float(v), int(max_wave_tiles),
+                             int(wave_stage_bytes))
         self._h = ctypes.c_void_p()
         st = lib().dtb_serve_create(self.ctx.handle, ctypes.byref(cfg), ctypes.byref(self._h))
         if st != 0:

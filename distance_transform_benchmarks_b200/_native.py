@@ -29,7 +29,8 @@ DTB_SYMBOLS = [
     "dtb_device_to_host", "dtb_context_set_tuning", "dtb_context_get_tuning", "dtb_plan_create", "dtb_plan_run",
     "dtb_plan_wait", "dtb_plan_autotune", "dtb_plan_destroy", "dtb_serve_create", "dtb_serve_submit", "dtb_serve_poll",
     "dtb_serve_release", "dtb_serve_get_stats", "dtb_serve_destroy", "dtb_gdt_ref_blocks", "dtb_image_alloc",
-    "dtb_image_free", "dtb_debug_inject_queue_stall", "dtb_image_read", "dtb_image_write",
+    "dtb_image_free", "dtb_debug_inject_queue_stall", "dtb_image_read", "dtb_image_write", "dtb_plan_get_tuning",
+    "dtb_context_set_tuning_cache",
 ]
 
 DTB_REQ_IMAGE = 0
@@ -64,11 +65,13 @@ class DtbStats(ctypes.Structure):
 
 
 class DtbTuning(ctypes.Structure):
-    _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32), ("host_chunk_kpx", ctypes.c_int32)]
+    _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32), ("host_chunk_kpx", ctypes.c_int32),
+                ("queue_buckets", ctypes.c_int32), ("bucket_width_pct", ctypes.c_int32), ("staging", ctypes.c_int32)]
 
 
 class DtbServeConfig(ctypes.Structure):
-    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_int32), ("v", ctypes.c_float)]
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_int32), ("v", ctypes.c_float),
+                ("max_wave_tiles", ctypes.c_uint32), ("wave_stage_bytes", ctypes.c_uint64)]
 
 
 class DtbServeRequest(ctypes.Structure):
@@ -84,7 +87,10 @@ class DtbServeCompletion(ctypes.Structure):
 class DtbServeStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int64) for n in ("submitted", "completed", "failed", "waves", "evictions", "pending",
                                              "resident_images")] + \
-               [(n, ctypes.c_uint64) for n in ("resident_bytes", "tiles", "tile_visits")]
+               [(n, ctypes.c_uint64) for n in ("resident_bytes", "tiles", "tile_visits")] + \
+               [(n, ctypes.c_double) for n in ("host_prep_ms", "copy_in_ms", "kernel_ms", "copy_out_ms", "queue_wait_ms",
+                                               "queue_wait_max_ms")] + \
+               [("waves_split", ctypes.c_int64)]
 
 
 class DtbError(RuntimeError):
@@ -151,6 +157,10 @@ def lib():
         L.dtb_plan_wait.argtypes = [P, P, ctypes.POINTER(DtbStats)]
         L.dtb_plan_autotune.restype = I32
         L.dtb_plan_autotune.argtypes = [P, P, I32, ctypes.POINTER(DtbTuning)]
+        L.dtb_plan_get_tuning.restype = I32
+        L.dtb_plan_get_tuning.argtypes = [P, ctypes.POINTER(DtbTuning)]
+        L.dtb_context_set_tuning_cache.restype = I32
+        L.dtb_context_set_tuning_cache.argtypes = [P, ctypes.c_char_p]
         L.dtb_plan_destroy.restype = None
         L.dtb_plan_destroy.argtypes = [P]
         L.dtb_serve_create.restype = I32

@@ -96,6 +96,50 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
   flush_stats(ws, q);
 }
 
+// Persistent tile worker that stages ahead (ns-mode): while a warp visits tile k it has the image box of its
+// next tile in flight into the other box of its slot.  The next tile comes from a non-blocking pop (an item a
+// pusher has already reserved); when there is none, the warp pops blocking after the visit, as the worker
+// above does.  A tile is claimed (PENDING -> RUNNING) only when its visit starts, so activations that reach
+// it while it waits are covered by that visit (it reads its halo after the claim) instead of forcing a re-run.
+template <int WPC, int MINB>
+__global__ void __launch_bounds__(WPC * 32, MINB)
+    ggdt_persistent_ahead(const ImgDesc* __restrict__ descs, const CUtensorMap* __restrict__ tmaps, uint32_t* states,
+                          Queue q) {
+  extern __shared__ uint8_t smem_raw[];
+  WarpSmemP& sm = warp_slot_p(smem_raw);
+  warp_slot_init(sm);
+  const QueueSched sch{q, states};
+  const int lane = threadIdx.x & 31;
+  WarpStats ws;
+  uint32_t pbits = 0;  // bit k: phase parity of box k's barrier; bit 2: the mask barrier's
+  uint32_t k = 0;      // box of the tile being visited
+  uint32_t cur = queue_pop(q);
+  if (cur != POP_NONE) stage_ahead(descs, tmaps, states, cur, sm.box[0], &sm.bar[0]);
+  while (cur != POP_NONE) {
+    uint32_t nxt = queue_try_pop(q);
+    if (nxt != POP_NONE) stage_ahead(descs, tmaps, states, nxt, sm.box[k ^ 1u], &sm.bar[k ^ 1u]);
+    uint32_t old = 0;
+    if (lane == 0) {
+      old = atomicXor(&states[cur], ST_PENDING | ST_RUNNING);
+      if (q.keys) q.keys[cur] = KEY_NONE;  // activations from here on belong to the next queue entry
+    }
+    old = __shfl_sync(~0u, old, 0);
+    const uint32_t img = old >> ST_IMG_SHIFT;
+    const ImgDesc dd = descs[img];
+    const VisitBufs vb{sm.box[k], sm.Wh, sm.Wv, &sm.bar[k], &sm.mbar, 1u << k, 4u, &pbits};
+    uint32_t nph, nact;
+    visit_ns<true>(dd, tmaps + 2 * img, tmaps + 2 * img + 1, cur, old, vb, sch, &nph, &nact);
+    count_visit(ws, q, nph, nact);
+    if (nxt == POP_NONE) {
+      nxt = queue_pop(q);
+      if (nxt != POP_NONE) stage_ahead(descs, tmaps, states, nxt, sm.box[k ^ 1u], &sm.bar[k ^ 1u]);
+    }
+    cur = nxt;
+    k ^= 1u;
+  }
+  flush_stats(ws, q);
+}
+
 // One host-driven round: one warp per tile, inactive tiles return at once.
 template <int MODE, int WPC>
 __global__ void __launch_bounds__(WPC * 32)
@@ -267,7 +311,7 @@ ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, u
   L.n = n;
   L.total = total;
   L.cap = next_pow2((uint32_t)std::min<uint64_t>(2ull * ((uint64_t)total + workers + 64u), 1ull << 31));
-  L.nb = buckets > 1 ? NBUCKET : 1u;
+  L.nb = std::max<uint32_t>(1u, std::min<uint32_t>(next_pow2(std::max<uint32_t>(buckets, 1u)), NBUCKET_MAX));
   size_t off = 0;
   L.o_hdr = off;    off = align_up(off + sizeof(QueueHdr), 256);
   L.o_states = off; off = align_up(off + 4ull * std::max<uint32_t>(total, 1), 256);
@@ -353,17 +397,24 @@ uint64_t tuning_key(int n, uint32_t total) {
   return ((uint64_t)next_pow2((uint32_t)std::max(n, 1)) << 32) | next_pow2(std::max<uint32_t>(total, 1));
 }
 
-Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns) {
+bool valid_policy(int buckets, float bucket_tiles) {
+  return buckets >= 1 && buckets <= (int)NBUCKET_MAX && (buckets & (buckets - 1)) == 0 && bucket_tiles > 0.0f &&
+         bucket_tiles <= 64.0f;
+}
+
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns, const LaunchTuning* t) {
   const uint64_t cap_visits = std::min<uint64_t>(0xF0000000ull, 4096ull * L.total + (1ull << 20));
   // A tile is re-visited only after a strict decrease of a neighbour's border; real inputs stay far below
   // this cap, which only turns a scheduling bug into an error instead of an endless run.
   Queue q{reinterpret_cast<QueueHdr*>(dbase + L.o_hdr), reinterpret_cast<uint32_t*>(dbase + L.o_ring), L.cap - 1,
           timeout_ns, (uint32_t)cap_visits, L.total};
-  if (L.nb > 1) {
-    q.nb_mask = L.nb - 1;
+  const uint32_t nb = t ? std::min<uint32_t>(L.nb, (uint32_t)t->buckets) : L.nb;
+  if (nb > 1) {
+    q.nb_mask = nb - 1;
     q.keys = reinterpret_cast<uint32_t*>(dbase + L.o_keys);
     q.wacc = reinterpret_cast<float*>(dbase + L.o_wacc);
   }
+  q.bucket_tiles = t ? t->bucket_tiles : DEFAULT_BUCKET_TILES;
   return q;
 }
 
@@ -381,7 +432,7 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
                               cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1, QueueHdr* fold) {
   const uint64_t stall_ns = ctx->inject_stall_ns;
   ctx->inject_stall_ns = 0;
-  Queue q = make_queue(dbase, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS);
+  Queue q = make_queue(dbase, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS, &t);
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(dbase + L.o_desc);
   const CUtensorMap* dtm = reinterpret_cast<const CUtensorMap*>(dbase + L.o_tmap);
   const uint32_t* dtile_base = reinterpret_cast<const uint32_t*>(dbase + L.o_base);
@@ -398,23 +449,31 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
     ggdt_phantom_pending<<<1, 1, 0, stream>>>(q.hdr);
     DTB_CUDA(ctx, cudaGetLastError());
   }
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(resident_workers(ctx, mode, t) / PERSIST_WPC);
-  cfg.blockDim = dim3(PERSIST_WPC * 32);
-  cfg.dynamicSmemBytes = PERSIST_SMEM;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
   if (ev0) DTB_CUDA(ctx, cudaEventRecord(ev0, stream));
-  void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
-  const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant] : (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
-  DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, fn, args));
+  dtb_status ls = launch_tile_kernel(ctx, mode, t, ddesc, dtm, states, q, stream);
+  if (ls != DTB_OK) return ls;
   if (ev1) DTB_CUDA(ctx, cudaEventRecord(ev1, stream));
   ggdt_finalize<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, n, total, states, q.hdr, fold);
   DTB_CUDA(ctx, cudaGetLastError());
+  return DTB_OK;
+}
+
+dtb_status launch_tile_kernel(dtb_context ctx, int mode, const LaunchTuning& t, const ImgDesc* descs,
+                              const CUtensorMap* tmaps, uint32_t* states, const Queue& q, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(resident_workers(ctx, mode, t) / PERSIST_WPC);
+  cfg.blockDim = dim3(PERSIST_WPC * 32);
+  cfg.dynamicSmemBytes = mode == MODE_NS ? ctx->ns_smem[t.variant] : PERSIST_SMEM;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;  // guarantees co-residency of all workers (the slot waits need it)
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  Queue qa = q;
+  void* args[4] = {(void*)&descs, (void*)&tmaps, (void*)&states, (void*)&qa};
+  const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant] : (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
+  DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, fn, args));
   return DTB_OK;
 }
 
@@ -565,7 +624,7 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   auto it = ctx->tuned.find(tuning_key(n, total));
   if (it != ctx->tuned.end()) tuning = it->second;
   const ScratchLayout L = layout_for(n, total, resident_workers(ctx, mode, tuning), rounds,
-                                     rounds ? 1u : NBUCKET);
+                                     rounds ? 1u : (uint32_t)tuning.buckets);
   if ((s = grow(ctx, &ctx->dscratch, &ctx->dscratch_size, L.bytes)) != DTB_OK) return s;
   uint8_t* dbase = reinterpret_cast<uint8_t*>(ctx->dscratch);
   if ((s = build_tables(ctx, jobs, L, ctx->hstage)) != DTB_OK) return s;
@@ -608,6 +667,15 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   ctx->async_pending = true;
   if ((flags & DTB_FLAG_ASYNC) && !host_io) return DTB_OK;
   return dtb_sync(ctx, stream);
+}
+
+void tuning_to_abi(dtb_context ctx, const LaunchTuning& lt, dtb_tuning* t) {
+  t->ctas_per_sm = NS_VARIANT_TABLE[lt.variant].ctas;
+  t->grid_percent = lt.grid_percent;
+  t->host_chunk_kpx = (int32_t)(ctx->host_chunk_px / 1024ull);
+  t->queue_buckets = lt.buckets;
+  t->bucket_width_pct = (int32_t)lrintf(lt.bucket_tiles * 100.0f);
+  t->staging = NS_VARIANT_TABLE[lt.variant].ahead ? 2 : 1;
 }
 
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr_dev, dtb_stats* st) {
@@ -668,6 +736,7 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
   if (!ctx) return DTB_ERR_OUT_OF_MEMORY;
   ctx->device = dev;
   ctx->num_sms = prop.multiProcessorCount;
+  ctx->gpu_name = prop.name;
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
@@ -680,16 +749,25 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
     delete ctx;
     return DTB_ERR_NO_DEVICE;
   }
-  ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[0]>;
-  ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[1]>;
-  ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, NS_VARIANT_CTAS[2]>;
+  static_assert(NS_VARIANT_TABLE[0].ctas == 2 && !NS_VARIANT_TABLE[0].ahead && NS_VARIANT_TABLE[1].ctas == 3 &&
+                    NS_VARIANT_TABLE[2].ctas == 4 && NS_VARIANT_TABLE[3].ctas == 2 && NS_VARIANT_TABLE[3].ahead &&
+                    NS_VARIANT_TABLE[4].ctas == 3 && NS_VARIANT_TABLE[4].ahead,
+                "kernel instantiations below follow NS_VARIANT_TABLE");
+  ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 2>;
+  ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 3>;
+  ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 4>;
+  ctx->ns_fn[3] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 2>;
+  ctx->ns_fn[4] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 3>;
   const void* kref = (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
   bool ok = true;
-  for (int k = 0; k < NS_VARIANTS && ok; ++k)
-    ok = cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
+  for (int k = 0; k < NS_VARIANTS && ok; ++k) {
+    ctx->ns_smem[k] = NS_VARIANT_TABLE[k].ahead ? PERSIST_SMEM_AHEAD : PERSIST_SMEM;
+    ok = cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->ns_smem[k]) ==
+             cudaSuccess &&
          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], PERSIST_WPC * 32,
-                                                       PERSIST_SMEM) == cudaSuccess &&
+                                                       ctx->ns_smem[k]) == cudaSuccess &&
          ctx->ns_blocks_per_sm[k] >= 1;
+  }
   ok = ok && cudaFuncSetAttribute(kref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ref_blocks_per_sm, kref, PERSIST_WPC * 32, PERSIST_SMEM) ==
            cudaSuccess &&
@@ -703,9 +781,13 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
     delete ctx;
     return DTB_ERR_NO_DEVICE;
   }
-  if (const char* e = getenv("DTB_NS_VARIANT")) {
+  if (const char* e = getenv("DTB_NS_VARIANT")) {  // index into NS_VARIANT_TABLE
     const int k = atoi(e);
     if (k >= 0 && k < NS_VARIANTS) ctx->tuning.variant = k;
+  }
+  if (const char* e = getenv("DTB_AUTOTUNE_CACHE")) {  // autotuner cache of earlier processes
+    ctx->tune_cache_path = e;
+    load_tuning_cache(ctx);
   }
   *out = ctx;
   return DTB_OK;
@@ -751,19 +833,27 @@ DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out) {
 
 DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t) {
   if (!ctx || !t) return DTB_ERR_INVALID_ARG;
-  int variant = ctx->tuning.variant;
-  if (t->ctas_per_sm != 0) {
-    variant = -1;
-    for (int k = 0; k < NS_VARIANTS; ++k)
-      if (NS_VARIANT_CTAS[k] == t->ctas_per_sm) variant = k;
-    if (variant < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "ctas_per_sm must be 2, 3 or 4");
-  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  LaunchTuning nt = ctx->tuning;
+  const NsVariant cur = NS_VARIANT_TABLE[nt.variant];
+  const int ctas = t->ctas_per_sm != 0 ? t->ctas_per_sm : cur.ctas;
+  const bool ahead = t->staging != 0 ? t->staging == 2 : cur.ahead;
+  if (t->staging < 0 || t->staging > 2) return fail(ctx, DTB_ERR_INVALID_ARG, "staging must be 1 or 2");
+  const int variant = ns_variant_of(ctas, ahead);
+  if (variant < 0)
+    return fail(ctx, DTB_ERR_INVALID_ARG, "ctas_per_sm must be 2, 3 or 4 (2 or 3 when the next tile is staged ahead)");
   const int pct = t->grid_percent == 0 ? 100 : t->grid_percent;
   if (pct < 1 || pct > 100) return fail(ctx, DTB_ERR_INVALID_ARG, "grid_percent must be in [1, 100]");
   if (t->host_chunk_kpx < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "host_chunk_kpx must be >= 0");
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  ctx->tuning.variant = variant;
-  ctx->tuning.grid_percent = pct;
+  const int buckets = t->queue_buckets != 0 ? t->queue_buckets : nt.buckets;
+  const float width = t->bucket_width_pct != 0 ? (float)t->bucket_width_pct / 100.0f : nt.bucket_tiles;
+  if (t->bucket_width_pct < 0 || !valid_policy(buckets, width))
+    return fail(ctx, DTB_ERR_INVALID_ARG, "queue_buckets must be 1, 2, 4, 8 or 16 and bucket_width_pct in 1..6400");
+  nt.variant = variant;
+  nt.grid_percent = pct;
+  nt.buckets = buckets;
+  nt.bucket_tiles = width;
+  ctx->tuning = nt;
   if (t->host_chunk_kpx > 0) ctx->host_chunk_px = (uint64_t)t->host_chunk_kpx * 1024ull;
   ctx->tuned.clear();
   return DTB_OK;
@@ -771,9 +861,7 @@ DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t) 
 
 DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t) {
   if (!ctx || !t) return DTB_ERR_INVALID_ARG;
-  t->ctas_per_sm = NS_VARIANT_CTAS[ctx->tuning.variant];
-  t->grid_percent = ctx->tuning.grid_percent;
-  t->host_chunk_kpx = (int32_t)(ctx->host_chunk_px / 1024ull);
+  tuning_to_abi(ctx, ctx->tuning, t);
   return DTB_OK;
 }
 

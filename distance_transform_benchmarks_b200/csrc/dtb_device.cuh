@@ -64,11 +64,11 @@ struct alignas(64) ImgDesc {
 };
 
 // Counters live on separate 128-byte lines.
-constexpr uint32_t NBUCKET = 8;  // priority buckets of the tile queue (power of two; swept 8 < 16 < 32)
+constexpr uint32_t NBUCKET_MAX = 16;  // priority buckets of the tile queue at most (the count is a power of two)
 struct alignas(128) Line { uint32_t v; uint32_t pad[31]; };
 struct QueueHdr {
-  Line heads[NBUCKET];  // next pop ticket, per bucket
-  Line tails[NBUCKET];  // next push position, per bucket
+  Line heads[NBUCKET_MAX];  // next pop ticket, per bucket
+  Line tails[NBUCKET_MAX];  // next push position, per bucket
   Line base;       // absolute index of the lowest bucket that may hold work (a hint: order is a heuristic)
   Line pending;    // tiles queued or running
   Line error;      // first device error code
@@ -79,9 +79,10 @@ struct QueueHdr {
   Line done;       // set once when pending reached 0
 };
 
-// The tile queue.  nb_mask = 0: one FIFO ring.  nb_mask = NBUCKET - 1: NBUCKET rings ordered by distance: an
+// The tile queue.  nb_mask = 0: one FIFO ring.  nb_mask = 2^k - 1 (k = 1..4): 2^k rings ordered by distance: an
 // activation carries the smallest value it can bring into the tile (a border distance plus an edge weight);
-// its bucket is that value in units of one tile-width of path cost of its image, relative to `base`.  Workers
+// its bucket is that value in units of `bucket_tiles` tile-widths of path cost of its image, relative to
+// `base`.  Workers
 // take from the lowest non-empty bucket, which approximates visiting tiles in order of distance (Dijkstra
 // order on the tile graph) and so avoids most re-visits of tiles reached first by a costlier path.  The map
 // does not depend on the order: every order ends in the same fixpoint.
@@ -95,6 +96,7 @@ struct Queue {
   uint32_t nb_mask = 0;     // bucket count - 1
   uint32_t* keys = nullptr;  // per tile: smallest pending activation value (float bits), KEY_NONE if none
   float* wacc = nullptr;     // per image: [sum, count] of the internal edge weights seen by first visits
+  float bucket_tiles = 0.5f; // bucket width in tile-widths of path cost (32 x the image's mean edge weight)
 };
 constexpr uint32_t KEY_NONE = 0xFFFFFFFFu;
 
@@ -109,6 +111,19 @@ struct alignas(128) WarpSmem {
   uint64_t bar;                              // TMA mbarrier
 };
 __device__ __forceinline__ uint8_t* mask_box(WarpSmem& sm) { return reinterpret_cast<uint8_t*>(sm.Wv); }
+
+// Per-warp shared memory of the staged-ahead tile kernel (17 KB: 12 warps per SM fit in 228 KB): the image
+// boxes of the tile being visited and of the warp's next tile, each the tile buffer B of its own visit once its
+// weights are computed; the weights; a barrier per box and one for the seed-mask box.
+constexpr int IMG_BOX_BYTES = IMG_BOX_ROWS * IMG_BOX_RGB;
+struct alignas(128) WarpSmemP {
+  uint8_t box[2][IMG_BOX_BYTES];
+  float Wh[TILE * W_STRIDE];
+  float Wv[(TILE + 1) * W_STRIDE];   // its first 1 KB receives the seed-mask TMA box before the weights
+  uint64_t bar[2];                   // image box k
+  uint64_t mbar;                     // seed-mask box
+};
+static_assert(TILE * W_STRIDE * 4 <= IMG_BOX_BYTES, "the tile buffer must fit an image box");
 
 // ------------------------------------------------------------------------------------------------------
 // PTX helpers
@@ -154,7 +169,7 @@ __device__ __forceinline__ void tmap_acquire(const CUtensorMap* map) {
 }
 
 // ------------------------------------------------------------------------------------------------------
-// Queue: one or NBUCKET ticket rings of tile ids (buckets ordered by distance) with one pending counter for
+// Queue: one or 2^k ticket rings of tile ids (buckets ordered by distance) with one pending counter for
 // termination.
 //   push: pending grows first, then a position of the item's bucket is reserved, then the item goes into its
 //         slot (the slot must be free: CAS from 0; a slot given back by a waiter is skipped).
@@ -332,6 +347,40 @@ __device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
     res = __shfl_sync(~0u, res, 0);
     if (res != POP_RESCAN) return res;
   }
+}
+
+// Non-blocking pop (whole warp) for staging a warp's next tile ahead: takes a ticket only in the lowest bucket
+// whose next item a pusher has already reserved (tail ahead of head, by CAS on the head, so no popper waits
+// there), so the wait for the slot write that follows is short and never for work that does not exist.
+// Returns the tile id, or POP_NONE when no reserved item was found (the caller then pops blocking later).
+__device__ __forceinline__ uint32_t queue_try_pop(const Queue& q) {
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (q.nb_mask) {
+    if (lane == 0) base = ld_volatile(&q.hdr->base.v);
+    base = __shfl_sync(~0u, base, 0);
+  }
+  const uint32_t bl = (base + (uint32_t)lane) & q.nb_mask;
+  uint32_t h = 0;
+  bool avail = false;
+  if ((uint32_t)lane <= q.nb_mask) {
+    h = ld_volatile(&q.hdr->heads[bl].v);
+    avail = (int32_t)(ld_volatile(&q.hdr->tails[bl].v) - h) > 0;
+  }
+  const uint32_t m = __ballot_sync(~0u, avail);
+  if (!m) return POP_NONE;
+  const int f = __ffs(m) - 1;
+  const uint32_t hf = __shfl_sync(~0u, h, f);
+  uint32_t res = POP_NONE;
+  if (lane == 0) {
+    const uint32_t b = (base + (uint32_t)f) & q.nb_mask;
+    if (atomicCAS(&q.hdr->heads[b].v, hf, hf + 1u) == hf) {
+      PopWatch w{globaltimer(), ld_volatile(&q.hdr->progress.v)};
+      res = slot_take(q, b, hf, w);  // tail > hf: the item is on its way, slot_take never gives the ticket back
+      if (res == POP_RESCAN) res = POP_NONE;
+    }
+  }
+  return __shfl_sync(~0u, res, 0);
 }
 
 // ------------------------------------------------------------------------------------------------------

@@ -221,7 +221,7 @@ dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_i
     std::vector<Job> cj(jobs.begin() + cut[k], jobs.begin() + cut[k + 1]);
     uint32_t total = 0;
     if ((s = count_tiles(ctx, cj, &total)) != DTB_OK) return s;
-    L[k] = layout_for((int)cj.size(), total, workers, false);
+    L[k] = layout_for((int)cj.size(), total, workers, false, (uint32_t)tuning.buckets);
     o_chunk[k] = soff;
     soff = align_up(soff + L[k].bytes, 256);
     for (int i = cut[k]; i < cut[k + 1]; ++i) {

@@ -19,11 +19,24 @@ namespace dtb {
 constexpr int PERSIST_WPC = 4;   // warps per CTA of the persistent tile kernel
 constexpr int ROUND_WPC = 4;
 constexpr size_t PERSIST_SMEM = PERSIST_WPC * sizeof(WarpSmem) + 128;
+constexpr size_t PERSIST_SMEM_AHEAD = PERSIST_WPC * sizeof(WarpSmemP) + 128;
 constexpr size_t ROUND_SMEM = ROUND_WPC * sizeof(WarpSmem) + 128;
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
-// ns-mode tile kernel variants: CTAs (of PERSIST_WPC warps) per SM, i.e. at most 255 / 168 / 128 registers.
-constexpr int NS_VARIANTS = 3;
-constexpr int NS_VARIANT_CTAS[NS_VARIANTS] = {2, 3, 4};
+// ns-mode tile kernel variants: CTAs (of PERSIST_WPC warps) per SM (at most 255 / 168 / 128 registers for
+// 2 / 3 / 4) and whether a warp stages its next tile ahead (17 KB of shared memory a warp instead of 13 KB, so
+// at most 3 CTAs per SM).
+struct NsVariant {
+  int ctas;
+  bool ahead;
+};
+constexpr int NS_VARIANTS = 5;
+constexpr NsVariant NS_VARIANT_TABLE[NS_VARIANTS] = {{2, false}, {3, false}, {4, false}, {2, true}, {3, true}};
+// Variant index of (ctas, ahead), or -1.
+inline int ns_variant_of(int ctas, bool ahead) {
+  for (int k = 0; k < NS_VARIANTS; ++k)
+    if (NS_VARIANT_TABLE[k].ctas == ctas && NS_VARIANT_TABLE[k].ahead == ahead) return k;
+  return -1;
+}
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -70,16 +83,22 @@ struct ScratchLayout {
   int n = 0;
   uint32_t total = 0;  // tiles
   uint32_t cap = 0;    // ring slots per bucket (power of two)
-  uint32_t nb = 1;     // priority buckets of the tile queue (1 or NBUCKET)
+  uint32_t nb = 1;     // priority-bucket rings allocated (a power of two <= NBUCKET_MAX; 1 = one FIFO ring)
   size_t o_hdr = 0, o_states = 0, o_ring = 0, o_keys = 0, o_wacc = 0, o_desc = 0, o_tmap = 0, o_base = 0, o_act = 0,
          o_chg = 0, bytes = 0;
   size_t ring_bytes() const { return 4ull * cap * nb; }
 };
 
-// Launch parameters of the tile kernel chosen for a run.
+// Queue policy defaults: 8 priority buckets half a tile-width of path cost wide.
+constexpr int DEFAULT_BUCKETS = 8;
+constexpr float DEFAULT_BUCKET_TILES = 0.5f;
+
+// Launch parameters of the tile kernel chosen for a run, and the policy of its tile queue.
 struct LaunchTuning {
-  int variant = 0;        // ns-mode kernel variant (index into NS_VARIANT_CTAS)
+  int variant = 0;        // ns-mode kernel variant (index into NS_VARIANT_TABLE)
   int grid_percent = 100; // share of the co-resident CTAs that is launched
+  int buckets = DEFAULT_BUCKETS;              // 1 = FIFO, else 2 / 4 / 8 / 16 distance-ordered buckets
+  float bucket_tiles = DEFAULT_BUCKET_TILES;  // bucket width in tile-widths of path cost
 };
 
 }  // namespace dtb
@@ -89,10 +108,13 @@ struct dtb_context_s {
   int num_sms = 0;
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   const void* ns_fn[dtb::NS_VARIANTS] = {};
+  size_t ns_smem[dtb::NS_VARIANTS] = {};
   int ns_blocks_per_sm[dtb::NS_VARIANTS] = {};
   int ref_blocks_per_sm = 0;
+  std::string gpu_name;                           // device name (key of the autotuner cache)
   dtb::LaunchTuning tuning;                       // default tuning of this context
   std::map<uint64_t, dtb::LaunchTuning> tuned;    // autotuner results by workload key
+  std::string tune_cache_path;                    // autotuner cache file (JSON), empty = none
   void* dscratch = nullptr;
   size_t dscratch_size = 0;
   void* dstage = nullptr;
@@ -158,8 +180,9 @@ dtb_status validate_view(dtb_context ctx, const dtb_image* im, const char* name,
 dtb_status check_triplet(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist, bool allow_rgb);
 
 // Scratch layout for n images with `total` tiles, `workers` resident warps; `rounds` adds the round flags;
-// `buckets`: priority buckets of the tile queue (NBUCKET for ns-mode runs, 1 = one FIFO ring).
-ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, uint32_t buckets = NBUCKET);
+// `buckets`: priority-bucket rings to allocate (a power of two <= NBUCKET_MAX; 1 = one FIFO ring).  A run may
+// use fewer buckets than its layout holds.
+ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, uint32_t buckets);
 // Enqueues the reset of the queue part of a scratch block (header, rings, activation keys, bucket widths).
 dtb_status reset_queue(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, cudaStream_t stream);
 // Host image of [descriptors | tensor maps | tile prefix] (bytes o_desc .. o_act of the layout).
@@ -173,6 +196,9 @@ uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t);
 // counters, added by finalize.
 dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, int mode, const LaunchTuning& t,
                               cudaStream_t stream, cudaEvent_t ev0, cudaEvent_t ev1, QueueHdr* fold = nullptr);
+// Enqueues the cooperative persistent tile kernel of `mode` under `t` (grid: resident_workers / PERSIST_WPC).
+dtb_status launch_tile_kernel(dtb_context ctx, int mode, const LaunchTuning& t, const ImgDesc* descs,
+                              const CUtensorMap* tmaps, uint32_t* states, const Queue& q, cudaStream_t stream);
 dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs, const dtb_image* const* imgs,
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream);
 // All images, masks and distances in host memory (ns-mode): chunked pipeline of 1-D host-to-device copies,
@@ -202,10 +228,20 @@ struct RepitchItem {
 // Failure self-test: counts one queued tile that is never pushed (the run ends on its no-progress limit).
 __global__ void ggdt_phantom_pending(QueueHdr* hdr);
 __global__ void __launch_bounds__(256) repitch_rows(const RepitchItem* __restrict__ items, int n, uint32_t total_rows);
-Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns = DEFAULT_TIMEOUT_NS);
+// The device queue of a scratch block; `t` (optional) selects the bucket count (at most the layout's) and width.
+Queue make_queue(uint8_t* dbase, const ScratchLayout& L, uint64_t timeout_ns = DEFAULT_TIMEOUT_NS,
+                 const LaunchTuning* t = nullptr);
+// Valid queue policy: buckets a power of two in [1, NBUCKET_MAX], width in (0, 64].
+bool valid_policy(int buckets, float bucket_tiles);
 // Workload key of the autotuner cache: image count and tile count, each rounded to a power of two.
 uint64_t tuning_key(int n, uint32_t total);
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr, dtb_stats* stats);
+// Autotuner cache file of the context (ctx->tune_cache_path): load this GPU's entries into ctx->tuned; write
+// one entry.  The caller holds ctx->mu.
+dtb_status load_tuning_cache(dtb_context ctx);
+dtb_status save_tuning_cache(dtb_context ctx, uint64_t key, const LaunchTuning& t, double ms);
+// The C ABI view of a launch tuning (host_chunk_kpx from the context).
+void tuning_to_abi(dtb_context ctx, const LaunchTuning& lt, dtb_tuning* t);
 // Reads and clears the status accumulated by host-pipeline calls since the last read (the caller synchronised).
 dtb_status finish_pipeline(dtb_context ctx);
 

@@ -18,7 +18,6 @@
 namespace dtb {
 
 constexpr int PHASE_LIMIT = 4096;
-constexpr float BUCKET_TILES = 0.5f;  // priority bucket width, in tile-widths of path cost (swept: 0.5 < 1 < 2)
 constexpr uint64_t TMA_TIMEOUT_NS = 2000000000ull;  // 2 s
 
 // ------------------------------------------------------------------------------------------------------
@@ -141,25 +140,76 @@ __device__ __forceinline__ float* dist_row(const ImgDesc& dd, int y) {
 // line an SM cached earlier can be returned.
 __device__ __forceinline__ float ld_dist(const ImgDesc& dd, int y, int x) { return __ldcg(dist_row(dd, y) + x); }
 
-// Waits for the TMA transactions of this warp's slot.  Bounded: after TMA_TIMEOUT_NS the error word is set
-// and the wait goes on for as long again, to give a slow copy the chance to land before the warp leaves; after
-// that the wait gives up, and a copy may then still be pending.  The error word ends the launch: every later
-// pop returns POP_NONE, so the warp issues no further copy and never waits on this barrier again.
-__device__ __forceinline__ bool tma_wait(WarpSmem& sm, uint32_t& parity, const Queue& q, uint32_t tile) {
+// Waits for the TMA transactions on `bar`; its phase parity is bit `pmask` of `pbits`.  Bounded: after
+// TMA_TIMEOUT_NS the error word is set and the wait goes on for as long again, to give a slow copy the chance
+// to land before the warp leaves; after that the wait gives up, and a copy may then still be pending.  The
+// error word ends the launch: every later pop returns POP_NONE, so the warp issues no further copy and never
+// waits on this barrier again.
+__device__ __forceinline__ bool tma_wait(uint64_t* bar, uint32_t& pbits, uint32_t pmask, const Queue& q, uint32_t tile) {
+  const uint32_t parity = (pbits & pmask) ? 1u : 0u;
   const uint64_t t0 = globaltimer();
   bool ok = true;
-  while (!mbar_try_wait(&sm.bar, parity)) {
+  while (!mbar_try_wait(bar, parity)) {
     const uint64_t dt = globaltimer() - t0;
     if (ok && dt > TMA_TIMEOUT_NS) { set_error(q, DERR_TMA_TIMEOUT, tile); ok = false; }
     if (dt > 2 * TMA_TIMEOUT_NS) break;
   }
-  parity ^= 1u;
+  pbits ^= pmask;
   return ok;
 }
 
-// Stages the image box (with 1-pixel halo) and, if needed, the seed-mask tile of a tile into shared memory.
-__device__ __forceinline__ void stage_tile(WarpSmem& sm, const CUtensorMap* tm_img, const CUtensorMap* tm_mask, bool rgb,
-                                           bool with_mask, int x0, int y0) {
+// Shared memory of one visit.  A self-staging visit loads its image box and seed-mask box on `bar`; a visit
+// staged ahead finds its image box issued on `bar` already and loads the mask box (seed visits only) on `mbar`.
+struct VisitBufs {
+  uint8_t* box;       // image box (TMA destination), the tile buffer B once the weights are computed
+  float* Wh;
+  float* Wv;          // its first 1 KB receives the seed-mask box before the weights
+  uint64_t* bar;
+  uint64_t* mbar;
+  uint32_t pmask;     // bit of *pbits holding bar's phase parity
+  uint32_t mmask;     // bit of *pbits holding mbar's phase parity
+  uint32_t* pbits;
+};
+
+__device__ __forceinline__ VisitBufs visit_bufs(WarpSmem& sm, uint32_t& pbits) {
+  return VisitBufs{sm.img, sm.Wh, sm.Wv, &sm.bar, &sm.bar, 1u, 1u, &pbits};
+}
+
+// Issues one 2-D TMA box into this warp's shared memory on `bar` (whole warp; lane 0 issues).  Orders this
+// warp's earlier generic accesses of the destination before the async-proxy writes.
+__device__ __forceinline__ void stage_box(void* dst, uint64_t* bar, const CUtensorMap* tm, uint32_t bytes, int x, int y) {
+  fence_proxy_async_smem();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    tmap_acquire(tm);
+    mbar_arrive_expect_tx(bar, bytes);
+    tma_load_2d(dst, tm, x, y, bar);
+  }
+}
+
+// The image box of a tile (1-pixel halo; x starts 16 bytes left of the halo so that it stays 16-byte aligned).
+__device__ __forceinline__ void stage_image_box(uint8_t* box, uint64_t* bar, const CUtensorMap* tm_img, bool rgb, int x0,
+                                                int y0) {
+  stage_box(box, bar, tm_img, (rgb ? IMG_BOX_RGB : IMG_BOX_GRAY) * IMG_BOX_ROWS, rgb ? 3 * x0 - 16 : x0 - 16, y0 - 1);
+}
+
+// Issues the image box of a warp's next tile ahead of its visit (the image index bits of a tile state never
+// change, so reading them before the tile is claimed is safe).
+__device__ __forceinline__ void stage_ahead(const ImgDesc* __restrict__ descs, const CUtensorMap* __restrict__ tmaps,
+                                            const uint32_t* states, uint32_t tile, uint8_t* box, uint64_t* bar) {
+  uint32_t st = 0;
+  if ((threadIdx.x & 31) == 0) st = ld_volatile(&states[tile]);
+  const uint32_t img = __shfl_sync(~0u, st, 0) >> ST_IMG_SHIFT;
+  const ImgDesc& dd = descs[img];
+  const uint32_t local = tile - dd.tile_base;
+  const uint32_t tx = local % (uint32_t)dd.tiles_x, ty = local / (uint32_t)dd.tiles_x;
+  stage_image_box(box, bar, tmaps + 2 * img, dd.channels == 3, (int)tx * TILE, (int)ty * TILE);
+}
+
+// Stages the image box (with 1-pixel halo) and, if needed, the seed-mask tile of a tile into shared memory,
+// both on vb.bar.
+__device__ __forceinline__ void stage_tile(const VisitBufs& vb, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
+                                           bool rgb, bool with_mask, int x0, int y0) {
   // Order this warp's earlier generic reads of the slot before the async-proxy writes below.
   fence_proxy_async_smem();
   __syncwarp();
@@ -167,9 +217,9 @@ __device__ __forceinline__ void stage_tile(WarpSmem& sm, const CUtensorMap* tm_i
     tmap_acquire(tm_img);
     if (with_mask) tmap_acquire(tm_mask);
     const uint32_t bytes = (rgb ? IMG_BOX_RGB : IMG_BOX_GRAY) * IMG_BOX_ROWS + (with_mask ? TILE * TILE : 0);
-    mbar_arrive_expect_tx(&sm.bar, bytes);
-    tma_load_2d(sm.img, tm_img, rgb ? 3 * x0 - 16 : x0 - 16, y0 - 1, &sm.bar);
-    if (with_mask) tma_load_2d(mask_box(sm), tm_mask, x0, y0, &sm.bar);
+    mbar_arrive_expect_tx(vb.bar, bytes);
+    tma_load_2d(vb.box, tm_img, rgb ? 3 * x0 - 16 : x0 - 16, y0 - 1, vb.bar);
+    if (with_mask) tma_load_2d(vb.Wv, tm_mask, x0, y0, vb.bar);
   }
 }
 
@@ -199,10 +249,10 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
 // row layout (immediate offsets from one base pointer per lane).
 // Returns the number of phases and activations through *nph / *nact.
 // ------------------------------------------------------------------------------------------------------
-template <class Sched>
+template <bool PRESTAGED, class Sched>
 __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
-                                         uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
-                                         const Sched& sch, uint32_t* nph_out, uint32_t* nact_out) {
+                                         uint32_t tile, uint32_t old_state, const VisitBufs& vb, const Sched& sch,
+                                         uint32_t* nph_out, uint32_t* nact_out) {
   const int lane = threadIdx.x & 31;
   const float INF = f_inf();
   const uint32_t local = tile - dd.tile_base;
@@ -216,7 +266,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   *nph_out = 0;
   *nact_out = 0;
 
-  stage_tile(sm, tm_img, tm_mask, rgb, seed, x0, y0);
+  if (!PRESTAGED) stage_tile(vb, tm_img, tm_mask, rgb, seed, x0, y0);
+  else if (seed) stage_box(vb.Wv, vb.mbar, tm_mask, TILE * TILE, x0, y0);
 
   // Neighbour states: lane 0 left, 1 right, 2 top, 3 bottom.
   const uint32_t nexist = (tx > 0 ? 1u : 0u) | (tx + 1 < dd.tiles_x ? 2u : 0u) | (ty > 0 ? 4u : 0u) |
@@ -250,20 +301,22 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
     for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
   }
 
-  if (!tma_wait(sm, parity, sch.q, tile)) return;
+  if (!tma_wait(vb.bar, *vb.pbits, vb.pmask, sch.q, tile)) return;
+  if (PRESTAGED && seed && !tma_wait(vb.mbar, *vb.pbits, vb.mmask, sch.q, tile)) return;
+  const uint8_t* mbox = reinterpret_cast<const uint8_t*>(vb.Wv);
 
   // Seeds first: the mask box shares memory with Wv.
   if (first) {
 #pragma unroll
     for (int y = 0; y < TILE; ++y) {
       const bool in = lane < vw && y < vh;
-      const bool s = seed && mask_box(sm)[y * TILE + lane] != 0;
+      const bool s = seed && mbox[y * TILE + lane] != 0;
       d[y] = in ? (s ? 0.0f : v) : INF;
     }
   } else if (seed) {
 #pragma unroll
     for (int y = 0; y < TILE; ++y)
-      if (lane < vw && y < vh && mask_box(sm)[y * TILE + lane] != 0) d[y] = 0.0f;
+      if (lane < vw && y < vh && mbox[y * TILE + lane] != 0) d[y] = 0.0f;
   }
   __syncwarp();
 
@@ -271,12 +324,12 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // are INF.
   {
     const float g2 = dd.g2;
-    const uint8_t* box = sm.img;
+    const uint8_t* box = vb.box;
     if (!rgb) {
       // Gray: the weight depends on |dI| in [0, 255] only.  A 256-entry table of the same expression (so the
       // same bits) costs 8 square roots per lane instead of 65; it sits in the part of the image box that the
       // 64-byte gray rows leave unused.
-      float* lut = reinterpret_cast<float*>(sm.img + GRAY_LUT_OFFSET);
+      float* lut = reinterpret_cast<float*>(vb.box + GRAY_LUT_OFFSET);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const uint32_t a = (uint32_t)(lane + 32 * k);
@@ -290,18 +343,18 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
         const int pcur = col[(y + 1) * IMG_BOX_GRAY];
         float w = lut[abs(pcur - pprev)];
         if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
-        sm.Wv[y * W_STRIDE + lane] = w;
+        vb.Wv[y * W_STRIDE + lane] = w;
         if (y < TILE) {
           float wx = lut[abs(pcur - (int)col[(y + 1) * IMG_BOX_GRAY - 1])];
           if (lane >= vw || y >= vh) wx = INF;
-          sm.Wh[y * W_STRIDE + lane] = wx;
+          vb.Wh[y * W_STRIDE + lane] = wx;
         }
         pprev = pcur;
       }
       const uint8_t* row = box + (lane + 1) * IMG_BOX_GRAY + 16;
       float er = lut[abs((int)row[TILE - 1] - (int)row[TILE])];
       if (lane >= vh || TILE - 1 >= vw) er = INF;
-      sm.Wh[lane * W_STRIDE + TILE] = er;
+      vb.Wh[lane * W_STRIDE + TILE] = er;
     } else {
       uint32_t pprev = box_pix(box, rgb, 0, lane);
 #pragma unroll 1
@@ -309,18 +362,18 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
         const uint32_t pcur = box_pix(box, rgb, y + 1, lane);
         float w = ns_weight(pprev, pcur, g2);
         if (lane >= vw || (y < TILE ? y >= vh : TILE - 1 >= vh)) w = INF;
-        sm.Wv[y * W_STRIDE + lane] = w;
+        vb.Wv[y * W_STRIDE + lane] = w;
         if (y < TILE) {
           float wx = ns_weight(box_pix(box, rgb, y + 1, lane - 1), pcur, g2);
           if (lane >= vw || y >= vh) wx = INF;
-          sm.Wh[y * W_STRIDE + lane] = wx;
+          vb.Wh[y * W_STRIDE + lane] = wx;
         }
         pprev = pcur;
       }
       // Edge (x = 31, x = 32) of row `lane`.
       float er = ns_weight(box_pix(box, rgb, lane + 1, TILE - 1), box_pix(box, rgb, lane + 1, TILE), g2);
       if (lane >= vh || TILE - 1 >= vw) er = INF;
-      sm.Wh[lane * W_STRIDE + TILE] = er;
+      vb.Wh[lane * W_STRIDE + TILE] = er;
     }
   }
   __syncwarp();
@@ -335,7 +388,7 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
       float wsum = 0.0f, wcnt = 0.0f;
 #pragma unroll 4
       for (int y = 1; y < TILE; ++y) {
-        const float w = sm.Wv[y * W_STRIDE + lane];
+        const float w = vb.Wv[y * W_STRIDE + lane];
         if (w < INF) { wsum += w; wcnt += 1.0f; }
       }
 #pragma unroll
@@ -349,11 +402,12 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
       }
     }
     const float s_ = *(volatile float*)&wa[0], c_ = *(volatile float*)&wa[1];
-    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (BUCKET_TILES * (float)TILE * s_) : 1.0f / (BUCKET_TILES * (float)TILE);
+    const float bt = sch.q.bucket_tiles;
+    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (bt * (float)TILE * s_) : 1.0f / (bt * (float)TILE);
   }
 
   // Local fixpoint.  B overlays the image box, which is no longer needed.
-  float* B = reinterpret_cast<float*>(sm.img);
+  float* B = reinterpret_cast<float*>(vb.box);
   // Start in the layout whose chains begin at the halo sides that can lower the tile now: a column phase
   // never reads the left / right halo, so a tile reached only from the side would spend its first column
   // phase without any effect.
@@ -364,10 +418,10 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
     for (int k = 0; k < TILE; ++k) pb[k * W_STRIDE] = d[k];
     __syncwarp();
     const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];
-    const bool hside = __any_sync(~0u, __fadd_rn(lft, sm.Wh[lane * W_STRIDE]) < dl ||
-                                           __fadd_rn(rgt, sm.Wh[lane * W_STRIDE + TILE]) < dr);
-    const bool vside = __any_sync(~0u, __fadd_rn(top, sm.Wv[lane]) < d[0] ||
-                                           __fadd_rn(bot, sm.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
+    const bool hside = __any_sync(~0u, __fadd_rn(lft, vb.Wh[lane * W_STRIDE]) < dl ||
+                                           __fadd_rn(rgt, vb.Wh[lane * W_STRIDE + TILE]) < dr);
+    const bool vside = __any_sync(~0u, __fadd_rn(top, vb.Wv[lane]) < d[0] ||
+                                           __fadd_rn(bot, vb.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
     if (hside && !vside) {
       col = false;
       const float* qb = B + lane * W_STRIDE;
@@ -381,15 +435,15 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   for (;;) {
     float wc[TILE + 1], wx[TILE];
     if (col) {  // element k of lane x: [k * 33 + x]
-      const float* pc = sm.Wv + lane;
-      const float* px = sm.Wh + lane;
+      const float* pc = vb.Wv + lane;
+      const float* px = vb.Wh + lane;
 #pragma unroll
       for (int k = 0; k <= TILE; ++k) wc[k] = pc[k * W_STRIDE];
 #pragma unroll
       for (int k = 0; k < TILE; ++k) wx[k] = px[k * W_STRIDE];
     } else {    // element k of lane y: [y * 33 + k]
-      const float* pc = sm.Wh + lane * W_STRIDE;
-      const float* px = sm.Wv + lane * W_STRIDE;
+      const float* pc = vb.Wh + lane * W_STRIDE;
+      const float* px = vb.Wv + lane * W_STRIDE;
 #pragma unroll
       for (int k = 0; k <= TILE; ++k) wc[k] = pc[k];
 #pragma unroll
@@ -432,8 +486,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   if (any || seed) {
     const float dt = B[lane], db = B[(TILE - 1) * W_STRIDE + lane];               // column layout
     const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];      // row layout
-    const float wt = sm.Wv[lane], wb = sm.Wv[TILE * W_STRIDE + lane];
-    const float wl = sm.Wh[lane * W_STRIDE], wr = sm.Wh[lane * W_STRIDE + TILE];
+    const float wt = vb.Wv[lane], wb = vb.Wv[TILE * W_STRIDE + lane];
+    const float wl = vb.Wh[lane * W_STRIDE], wr = vb.Wh[lane * W_STRIDE + TILE];
     // The activation value of a side: the smallest border value it can bring (its priority in the queue).
     const float vl = __fadd_rn(dl, wl), vr = __fadd_rn(dr, wr), vt = __fadd_rn(dt, wt), vb = __fadd_rn(db, wb);
     const uint32_t kl = __reduce_min_sync(~0u, vl < lft ? __float_as_uint(vl) : KEY_NONE);
@@ -503,7 +557,8 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   const float v = dd.v, le = dd.l_eucl, lg = dd.l_grad;
   const float sq2 = 1.41421354f;  // sqrtf(2.f), reference generalised_distance_transform.cu:111
 
-  stage_tile(sm, tm_img, tm_mask, false, seed, x0, y0);
+  const VisitBufs vb = visit_bufs(sm, parity);
+  stage_tile(vb, tm_img, tm_mask, false, seed, x0, y0);
 
   // Neighbour k = lane (0..7): (dx, dy) = L, R, T, B, TL, TR, BL, BR.
   const int ndx[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
@@ -550,7 +605,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
     for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
   }
 
-  if (!tma_wait(sm, parity, sch.q, tile)) return;
+  if (!tma_wait(&sm.bar, parity, 1u, sch.q, tile)) return;
 
   // Padded copy of the image box: pimg[r * 36 + c + 1] = pixel (tile column c, box row r), c = -1..32.
   uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.Wh + 96);  // 34 * 36 = 1224 bytes after the halo rows
@@ -613,7 +668,8 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
       }
     }
     const float s_ = *(volatile float*)&wa[0], c_ = *(volatile float*)&wa[1];
-    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (BUCKET_TILES * (float)TILE * s_) : 1.0f / (BUCKET_TILES * (float)TILE);
+    const float bt = sch.q.bucket_tiles;
+    inv_width = (c_ > 0.0f && s_ > 0.0f) ? c_ / (bt * (float)TILE * s_) : 1.0f / (bt * (float)TILE);
   }
 
   bool any = false;
@@ -797,7 +853,7 @@ __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap*
   const CUtensorMap* tm_mask = tmaps + 2 * img + 1;
   uint32_t nph, nact;
   if (MODE == MODE_NS)
-    visit_ns(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
+    visit_ns<false>(dd, tm_img, tm_mask, tile, old_state, visit_bufs(sm, parity), sch, &nph, &nact);
   else if (dd.ref_fma)
     visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
   else
@@ -813,6 +869,21 @@ __device__ __forceinline__ WarpSmem& warp_slot(uint8_t* smem_raw) {
 __device__ __forceinline__ void warp_slot_init(WarpSmem& sm) {
   if ((threadIdx.x & 31) == 0) {
     mbar_init(&sm.bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ WarpSmemP& warp_slot_p(uint8_t* smem_raw) {
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  return reinterpret_cast<WarpSmemP*>(base)[threadIdx.x >> 5];
+}
+
+__device__ __forceinline__ void warp_slot_init(WarpSmemP& sm) {
+  if ((threadIdx.x & 31) == 0) {
+    mbar_init(&sm.bar[0], 1);
+    mbar_init(&sm.bar[1], 1);
+    mbar_init(&sm.mbar, 1);
     fence_mbar_init();
   }
   __syncwarp();

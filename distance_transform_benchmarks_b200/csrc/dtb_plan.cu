@@ -1,9 +1,15 @@
 // dtb_plan.cu -- batch plans: a ragged ns-mode batch prepared once, captured in a CUDA graph, run many times;
-// and the autotuner that picks the tile-kernel launch variant for a batch.
+// the autotuner that picks the tile-kernel variant (CTAs per SM, staging), grid share and tile-queue policy
+// (FIFO or distance-ordered buckets, their count and width) for a batch; and its JSON cache, keyed by GPU
+// name and workload size class, which later processes reuse.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "dtb.h"
@@ -55,7 +61,138 @@ bool aligned16(const dtb_image* im) {
   return (reinterpret_cast<uintptr_t>(im->buffer) & 15u) == 0 && (im->pitch & 15) == 0;
 }
 
+// ---- autotuner cache: {"format": "dtb-autotune-1", "entries": [{"gpu": ..., "images_pow2": ..., ...}, ...]} ----
+struct CacheEntry {
+  std::string gpu;
+  uint64_t images = 0, tiles = 0;
+  int ctas = 0, staging = 0, grid = 0, buckets = 0, width_pct = 0;
+  double ms = 0.0;
+};
+
+// Parses the flat entry objects of a cache file (string and number values only, as written below).
+std::vector<CacheEntry> parse_cache(const std::string& text) {
+  std::vector<CacheEntry> out;
+  size_t i = text.find("\"entries\"");
+  if (i == std::string::npos) return out;
+  i = text.find('[', i);
+  while (i != std::string::npos) {
+    const size_t o = text.find('{', i), e = text.find('}', o == std::string::npos ? i : o);
+    if (o == std::string::npos || e == std::string::npos) break;
+    CacheEntry c;
+    size_t k = o + 1;
+    while (k < e) {
+      const size_t q0 = text.find('"', k);
+      if (q0 == std::string::npos || q0 >= e) break;
+      const size_t q1 = text.find('"', q0 + 1);
+      const size_t colon = text.find(':', q1);
+      if (q1 == std::string::npos || colon == std::string::npos || colon >= e) break;
+      const std::string key = text.substr(q0 + 1, q1 - q0 - 1);
+      size_t v = colon + 1;
+      while (v < e && std::isspace((unsigned char)text[v])) ++v;
+      std::string val;
+      if (v < e && text[v] == '"') {
+        const size_t v1 = text.find('"', v + 1);
+        if (v1 == std::string::npos || v1 > e) break;
+        val = text.substr(v + 1, v1 - v - 1);
+        k = v1 + 1;
+      } else {
+        size_t v1 = v;
+        while (v1 < e && text[v1] != ',' && !std::isspace((unsigned char)text[v1])) ++v1;
+        val = text.substr(v, v1 - v);
+        k = v1;
+      }
+      if (key == "gpu") c.gpu = val;
+      else if (key == "images_pow2") c.images = std::strtoull(val.c_str(), nullptr, 10);
+      else if (key == "tiles_pow2") c.tiles = std::strtoull(val.c_str(), nullptr, 10);
+      else if (key == "ctas_per_sm") c.ctas = std::atoi(val.c_str());
+      else if (key == "staging") c.staging = std::atoi(val.c_str());
+      else if (key == "grid_percent") c.grid = std::atoi(val.c_str());
+      else if (key == "queue_buckets") c.buckets = std::atoi(val.c_str());
+      else if (key == "bucket_width_pct") c.width_pct = std::atoi(val.c_str());
+      else if (key == "ms") c.ms = std::atof(val.c_str());
+    }
+    out.push_back(c);
+    i = e + 1;
+    if (text.find('{', i) == std::string::npos) break;
+  }
+  return out;
+}
+
+bool read_file(const std::string& path, std::string* out) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  char buf[4096];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof(buf), f)) > 0) out->append(buf, n);
+  std::fclose(f);
+  return true;
+}
+
+uint64_t key_of(const CacheEntry& c) { return (c.images << 32) | c.tiles; }
+
 }  // namespace
+
+namespace dtb {
+
+// Entries of this context's GPU whose fields are valid go into ctx->tuned (the caller holds ctx->mu).
+dtb_status load_tuning_cache(dtb_context ctx) {
+  std::string text;
+  if (!read_file(ctx->tune_cache_path, &text)) return DTB_OK;  // no cache yet
+  for (const CacheEntry& c : parse_cache(text)) {
+    if (c.gpu != ctx->gpu_name) continue;
+    const int v = ns_variant_of(c.ctas, c.staging == 2);
+    if (v < 0 || c.grid < 1 || c.grid > 100 || !valid_policy(c.buckets, (float)c.width_pct / 100.0f)) continue;
+    LaunchTuning t;
+    t.variant = v;
+    t.grid_percent = c.grid;
+    t.buckets = c.buckets;
+    t.bucket_tiles = (float)c.width_pct / 100.0f;
+    ctx->tuned[key_of(c)] = t;
+  }
+  return DTB_OK;
+}
+
+// Rewrites the cache file with the entry of (this GPU, key) replaced by t (other entries kept); written to a
+// temporary file first and renamed, so readers never see a partial file (the caller holds ctx->mu).
+dtb_status save_tuning_cache(dtb_context ctx, uint64_t key, const LaunchTuning& t, double ms) {
+  std::string text;
+  std::vector<CacheEntry> entries;
+  if (read_file(ctx->tune_cache_path, &text)) entries = parse_cache(text);
+  CacheEntry n;
+  n.gpu = ctx->gpu_name;
+  n.images = key >> 32;
+  n.tiles = key & 0xFFFFFFFFull;
+  n.ctas = NS_VARIANT_TABLE[t.variant].ctas;
+  n.staging = NS_VARIANT_TABLE[t.variant].ahead ? 2 : 1;
+  n.grid = t.grid_percent;
+  n.buckets = t.buckets;
+  n.width_pct = (int)lrintf(t.bucket_tiles * 100.0f);
+  n.ms = ms;
+  bool replaced = false;
+  for (CacheEntry& c : entries)
+    if (c.gpu == n.gpu && key_of(c) == key) {
+      c = n;
+      replaced = true;
+    }
+  if (!replaced) entries.push_back(n);
+  const std::string tmp = ctx->tune_cache_path + ".tmp";
+  FILE* f = std::fopen(tmp.c_str(), "wb");
+  if (!f) return fail(ctx, DTB_ERR_IO, "cannot write %s", tmp.c_str());
+  std::fprintf(f, "{\"format\": \"dtb-autotune-1\", \"entries\": [");
+  for (size_t i = 0; i < entries.size(); ++i) {
+    const CacheEntry& c = entries[i];
+    std::fprintf(f,
+                 "%s\n  {\"gpu\": \"%s\", \"images_pow2\": %llu, \"tiles_pow2\": %llu, \"ctas_per_sm\": %d, \"staging\": %d, "
+                 "\"grid_percent\": %d, \"queue_buckets\": %d, \"bucket_width_pct\": %d, \"ms\": %.4f}",
+                 i ? "," : "", c.gpu.c_str(), (unsigned long long)c.images, (unsigned long long)c.tiles, c.ctas, c.staging,
+                 c.grid, c.buckets, c.width_pct, c.ms);
+  }
+  std::fprintf(f, "\n]}\n");
+  const bool ok = std::fclose(f) == 0 && std::rename(tmp.c_str(), ctx->tune_cache_path.c_str()) == 0;
+  return ok ? DTB_OK : fail(ctx, DTB_ERR_IO, "cannot write %s", ctx->tune_cache_path.c_str());
+}
+
+}  // namespace dtb
 
 extern "C" {
 
@@ -98,7 +235,7 @@ DTB_API dtb_status dtb_plan_create(dtb_context ctx, int32_t n, const dtb_image* 
   // The ring must hold every resident warp of any variant the autotuner may pick.
   uint32_t workers = 0;
   for (int k = 0; k < NS_VARIANTS; ++k) workers = std::max(workers, resident_workers(ctx, MODE_NS, LaunchTuning{k, 100}));
-  p->L = layout_for(n, total, workers, false);
+  p->L = layout_for(n, total, workers, false, NBUCKET_MAX);  // room for every queue policy of the autotuner
   p->key = tuning_key(n, total);
   auto it = ctx->tuned.find(p->key);
   p->tuning = it != ctx->tuned.end() ? it->second : ctx->tuning;
@@ -143,32 +280,66 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
   cudaEvent_t a, b;
   DTB_CUDA(ctx, cudaEventCreate(&a));
   DTB_CUDA(ctx, cudaEventCreate(&b));
-  static const int kPercent[3] = {100, 75, 50};
   float best_ms = INFINITY;
   LaunchTuning best = p->tuning;
   dtb_status s = DTB_OK;
-  for (int v = 0; v < NS_VARIANTS && s == DTB_OK; ++v) {
-    for (int pc = 0; pc < 3 && s == DTB_OK; ++pc) {
-      p->tuning = LaunchTuning{v, kPercent[pc]};
-      if ((s = capture(p)) != DTB_OK) break;
-      if ((s = dtb_plan_run(p, stream)) != DTB_OK || (s = dtb_plan_wait(p, stream, nullptr)) != DTB_OK) break;
-      std::vector<float> t;
-      for (int r = 0; r < reps && s == DTB_OK; ++r) {
-        cudaEventRecord(a, st);
-        s = dtb_plan_run(p, stream);
-        cudaEventRecord(b, st);
-        if (s == DTB_OK) s = dtb_plan_wait(p, stream, nullptr);
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, a, b);
-        t.push_back(ms);
+  // Median time of `reps` graph runs under tuning t (after one untimed run); keeps the fastest.
+  auto trial = [&](const LaunchTuning& t) {
+    if (s != DTB_OK) return;
+    p->tuning = t;
+    if ((s = capture(p)) != DTB_OK) return;
+    if ((s = dtb_plan_run(p, stream)) != DTB_OK || (s = dtb_plan_wait(p, stream, nullptr)) != DTB_OK) return;
+    std::vector<float> ts;
+    for (int r = 0; r < reps && s == DTB_OK; ++r) {
+      cudaEventRecord(a, st);
+      s = dtb_plan_run(p, stream);
+      cudaEventRecord(b, st);
+      if (s == DTB_OK) s = dtb_plan_wait(p, stream, nullptr);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, a, b);
+      ts.push_back(ms);
+    }
+    if (s != DTB_OK) return;
+    std::sort(ts.begin(), ts.end());
+    const float med = ts[ts.size() / 2];
+    if (med < best_ms) {
+      best_ms = med;
+      best = t;
+    }
+  };
+  // Coordinate search: (1) kernel variant x grid share under the current queue policy; (2) queue policy
+  // (FIFO; 8 or 16 buckets of 1/4, 1/2 or 1 tile-width) under the best launch; (3) the variants again under the
+  // best policy.
+  static const int kPercent[3] = {100, 75, 50};
+  const LaunchTuning start = p->tuning;
+  for (int v = 0; v < NS_VARIANTS; ++v)
+    for (int pc = 0; pc < 3; ++pc) {
+      LaunchTuning t = start;
+      t.variant = v;
+      t.grid_percent = kPercent[pc];
+      trial(t);
+    }
+  {
+    const LaunchTuning launch = best;
+    LaunchTuning t = launch;
+    t.buckets = 1;
+    trial(t);
+    static const int kBuckets[2] = {8, 16};
+    static const float kWidth[3] = {0.25f, 0.5f, 1.0f};
+    for (int nb : kBuckets)
+      for (float w : kWidth) {
+        t = launch;
+        t.buckets = nb;
+        t.bucket_tiles = w;
+        trial(t);
       }
-      if (s != DTB_OK) break;
-      std::sort(t.begin(), t.end());
-      const float med = t[t.size() / 2];
-      if (med < best_ms) {
-        best_ms = med;
-        best = p->tuning;
-      }
+  }
+  {
+    const LaunchTuning policy = best;
+    for (int v = 0; v < NS_VARIANTS; ++v) {
+      LaunchTuning t = policy;
+      t.variant = v;
+      trial(t);
     }
   }
   cudaEventDestroy(a);
@@ -179,13 +350,24 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
   {
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->tuned[p->key] = best;
+    if (!ctx->tune_cache_path.empty()) save_tuning_cache(ctx, p->key, best, best_ms);
   }
-  if (chosen) {
-    chosen->ctas_per_sm = NS_VARIANT_CTAS[best.variant];
-    chosen->grid_percent = best.grid_percent;
-    chosen->host_chunk_kpx = (int32_t)(ctx->host_chunk_px / 1024ull);
-  }
+  if (chosen) tuning_to_abi(ctx, best, chosen);
   return DTB_OK;
+}
+
+DTB_API dtb_status dtb_plan_get_tuning(dtb_plan p, dtb_tuning* out) {
+  if (!p || !out) return DTB_ERR_INVALID_ARG;
+  tuning_to_abi(p->ctx, p->tuning, out);
+  return DTB_OK;
+}
+
+DTB_API dtb_status dtb_context_set_tuning_cache(dtb_context ctx, const char* path) {
+  if (!ctx) return DTB_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->tune_cache_path = path ? path : "";
+  if (ctx->tune_cache_path.empty()) return DTB_OK;
+  return load_tuning_cache(ctx);
 }
 
 DTB_API void dtb_plan_destroy(dtb_plan p) {

@@ -165,9 +165,20 @@ struct Request {
 
 size_t plane_pitch(size_t row_bytes) { return row_bytes % 16 ? align_up(row_bytes, 128) : row_bytes; }
 
+uint64_t tiles_of(int W, int H) { return (uint64_t)((W + 31) / 32) * (uint64_t)((H + 31) / 32); }
+
+// Device staging a new image needs in a wave: its image and mask planes, where their rows need a new pitch.
+size_t stage_need(int W, int H, int C) {
+  size_t b = 0;
+  if (plane_pitch((size_t)W * C) != (size_t)W * C) b += align_up((size_t)W * C * H, 256);
+  if (plane_pitch((size_t)W) != (size_t)W) b += align_up((size_t)W * H, 256);
+  return b;
+}
+
 }  // namespace
 
-// Device and pinned host buffers of one wave in flight; a slot is reused only after its previous wave ended.
+// Device and pinned host buffers of one wave in flight, allocated by dtb_serve_create for the per-wave limits;
+// a slot is reused only after its previous wave ended.
 struct WaveSlot {
   void* scratch = nullptr;  // queue, tile states, tables of the wave
   size_t scratch_size = 0;
@@ -176,7 +187,15 @@ struct WaveSlot {
   uint8_t* hpin = nullptr;  // pinned host copy of the wave's tables
   size_t hpin_size = 0;
   cudaEvent_t ev_in = nullptr, ev_comp = nullptr, ev_done = nullptr;
+  // Timing of the wave's phases on their streams: copies in, tile run, copies out (start and end of each).
+  cudaEvent_t t_in0 = nullptr, t_in1 = nullptr, t_run0 = nullptr, t_run1 = nullptr, t_out0 = nullptr, t_out1 = nullptr;
 };
+
+// Per-wave limits (dtb_serve_config defaults).
+constexpr int SERVE_MAX_WAVE_REQUESTS = 4096;
+constexpr uint32_t SERVE_MAX_WAVE_TILES = 1u << 20;
+constexpr uint64_t SERVE_WAVE_STAGE_BYTES = 256ull << 20;
+constexpr size_t SERVE_MAX_WAVE_DISKS = 65536;
 
 struct dtb_server_s {
   dtb_context ctx = nullptr;
@@ -197,6 +216,12 @@ struct dtb_server_s {
   WaveSlot slot[2];
   cudaStream_t s_in = nullptr, s_run = nullptr, s_out = nullptr;  // copies in, tile runs, copies out
   dtb_serve_stats st{};
+  // Per-wave limits, and the queue geometry every wave's scratch was sized for.
+  int max_reqs = SERVE_MAX_WAVE_REQUESTS;
+  uint32_t max_tiles = SERVE_MAX_WAVE_TILES;
+  size_t stage_cap = SERVE_WAVE_STAGE_BYTES;
+  uint32_t workers = 0;  // resident warps of the largest tile-kernel launch
+  uint32_t nb = 1;       // priority buckets of the waves' tile queues
 };
 
 namespace {
@@ -239,16 +264,23 @@ bool make_room(dtb_server s, size_t bytes, size_t* off) {
   return true;
 }
 
-// Admission of one wave (caller holds mu).  Requests that cannot run now stay pending in order.
-std::vector<Request> admit(dtb_server s) {
+// Admission of one wave (caller holds mu).  Requests that cannot run now stay pending in order.  The wave is
+// closed when the next request would take it past a per-wave limit (requests, tiles, staging, disks): the
+// buffers of a wave slot were sized for those limits at create time.  *split reports such a close.
+std::vector<Request> admit(dtb_server s, bool* split) {
   std::vector<Request> wave;
   std::deque<Request> keep;
   const auto now = Clock::now();
   bool blocked = false;  // a new image that did not fit keeps later new images waiting (arrival order)
+  bool closed = false;   // a per-wave limit was reached: the rest waits for the next wave
+  uint64_t w_tiles = 0;
+  size_t w_stage = 0, w_disks = 0;
+  *split = false;
   while (!s->pending.empty()) {
     Request q = std::move(s->pending.front());
     s->pending.pop_front();
-    if (s->cfg.max_wave_requests > 0 && (int32_t)wave.size() >= s->cfg.max_wave_requests) {
+    if (closed || (int32_t)wave.size() >= s->max_reqs) {
+      if (!closed) closed = *split = true;
       keep.push_back(std::move(q));
       continue;
     }
@@ -262,6 +294,15 @@ std::vector<Request> admit(dtb_server s) {
         keep.push_back(std::move(q));  // one wave in flight per image: its map may still be on its way out
         continue;
       }
+      const uint64_t t = tiles_of(it->second.W, it->second.H);
+      const size_t nd = q.disks.size() / 3;
+      if (!wave.empty() && (w_tiles + t > s->max_tiles || w_disks + nd > SERVE_MAX_WAVE_DISKS)) {
+        closed = *split = true;
+        keep.push_back(std::move(q));
+        continue;
+      }
+      w_tiles += t;
+      w_disks += nd;
       it->second.wave = s->wave_no;
       it->second.last_use = ++s->tick;
       wave.push_back(std::move(q));
@@ -273,6 +314,17 @@ std::vector<Request> admit(dtb_server s) {
       continue;
     }
     if (blocked) {
+      keep.push_back(std::move(q));
+      continue;
+    }
+    const uint64_t t = tiles_of(q.r.img.width, q.r.img.height);
+    const size_t sb = stage_need(q.r.img.width, q.r.img.height, q.r.img.elem_size);
+    if (t > s->max_tiles || sb > s->stage_cap) {
+      complete(s, q, DTB_ERR_CAPACITY, now);  // larger than a whole wave may be
+      continue;
+    }
+    if (!wave.empty() && (w_tiles + t > s->max_tiles || w_stage + sb > s->stage_cap)) {
+      closed = *split = true;
       keep.push_back(std::move(q));
       continue;
     }
@@ -302,10 +354,26 @@ std::vector<Request> admit(dtb_server s) {
     r.wave = s->wave_no;
     r.last_use = ++s->tick;
     s->resident[q.r.image_id] = r;
+    w_tiles += t;
+    w_stage += sb;
     wave.push_back(std::move(q));
   }
   s->pending = std::move(keep);
   return wave;
+}
+
+// Device scratch a wave of n requests and `total` tiles needs: its run layout plus warm flags, disks and
+// repitch items; *o_* receive the offsets of the three extras.
+size_t wave_scratch_bytes(const ScratchLayout& L, int n, size_t ndisks, size_t nitems, size_t* o_warm, size_t* o_disks,
+                          size_t* o_items) {
+  size_t off = L.bytes;
+  *o_warm = off;
+  off = align_up(off + (size_t)std::max(n, 1), 256);
+  *o_disks = off;
+  off = align_up(off + sizeof(DiskItem) * std::max<size_t>(ndisks, 1), 256);
+  *o_items = off;
+  off = align_up(off + sizeof(RepitchItem) * std::max<size_t>(nitems, 1), 256);
+  return off;
 }
 
 // A wave in flight: its requests, slot and device queue header.
@@ -315,6 +383,7 @@ struct InFlight {
   int64_t no = 0;
   uint32_t total = 0;
   const QueueHdr* hdr = nullptr;
+  double prep_ms = 0.0;  // host time to admit and enqueue the wave
 };
 
 // Enqueues one wave: copies in and table upload on s_in, tile work on s_run, copies out on s_out; ev_done of
@@ -371,9 +440,11 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
       }
     }
   }
-  dtb_status s2 = grow(ctx, &ws.stage, &ws.stage_size, std::max<size_t>(stage_bytes, 256));
-  if (s2 != DTB_OK) return s2;
+  dtb_status s2 = DTB_OK;
+  if (stage_bytes > ws.stage_size)  // admission keeps a wave within the slot's staging
+    return fail(ctx, DTB_ERR_CAPACITY, "serve: wave staging %zu > %zu bytes", stage_bytes, ws.stage_size);
   uint8_t* stage = static_cast<uint8_t*>(ws.stage);
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_in0, s->s_in));
   // Host -> device: one 1-D copy per plane (into the resident plane, or into staging + repitch).
   for (int i = 0; i < n; ++i) {
     if (warm[i]) continue;
@@ -402,33 +473,21 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
   // Scratch: run layout + warm flags + disks + repitch items, one upload.
   uint32_t total = 0;
   if ((s2 = count_tiles(ctx, jobs, &total)) != DTB_OK) return s2;
-  const LaunchTuning tuning = ctx->tuning;
-  const ScratchLayout L = layout_for(n, total, resident_workers(ctx, MODE_NS, tuning), false);
-  size_t off = L.bytes;
-  const size_t o_warm = off;
-  off = align_up(off + (size_t)std::max(n, 1), 256);
-  const size_t o_disks = off;
-  off = align_up(off + sizeof(DiskItem) * std::max<size_t>(disks.size(), 1), 256);
-  const size_t o_items = off;
-  off = align_up(off + sizeof(RepitchItem) * std::max<size_t>(items.size(), 1), 256);
-  if ((s2 = grow(ctx, &ws.scratch, &ws.scratch_size, off)) != DTB_OK) return s2;
+  LaunchTuning tuning = ctx->tuning;
+  tuning.buckets = (int)std::min<uint32_t>((uint32_t)tuning.buckets, s->nb);
+  const ScratchLayout L = layout_for(n, total, s->workers, false, s->nb);
+  size_t o_warm = 0, o_disks = 0, o_items = 0;
+  const size_t off = wave_scratch_bytes(L, n, disks.size(), items.size(), &o_warm, &o_disks, &o_items);
+  if (off > ws.scratch_size)  // admission keeps a wave within the slot's scratch
+    return fail(ctx, DTB_ERR_CAPACITY, "serve: wave scratch %zu > %zu bytes", off, ws.scratch_size);
   uint8_t* sc = static_cast<uint8_t*>(ws.scratch);
   std::vector<uint8_t> tab;
   if ((s2 = build_tables(ctx, jobs, L, tab)) != DTB_OK) return s2;
   // Tables, warm flags, disks and repitch items: one upload from the slot's pinned buffer (free: the slot's
   // previous wave has ended), so that the copy does not wait for the other wave's work.
   const size_t hbytes = off - L.o_desc;
-  if (ws.hpin_size < hbytes) {
-    if (ws.hpin) cudaFreeHost(ws.hpin);
-    ws.hpin = nullptr;
-    ws.hpin_size = 0;
-    const size_t sz = align_up(hbytes + hbytes / 4, 1 << 16);
-    if (cudaHostAlloc((void**)&ws.hpin, sz, cudaHostAllocDefault) != cudaSuccess) {
-      ws.hpin = nullptr;
-      return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "cudaHostAlloc(serve tables) failed");
-    }
-    ws.hpin_size = sz;
-  }
+  if (ws.hpin_size < hbytes)
+    return fail(ctx, DTB_ERR_CAPACITY, "serve: wave tables %zu > %zu bytes", hbytes, ws.hpin_size);
   uint8_t* host = ws.hpin;
   std::memset(host, 0, hbytes);
   std::copy(tab.begin(), tab.end(), host);
@@ -438,8 +497,10 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
   std::copy(reinterpret_cast<const uint8_t*>(items.data()), reinterpret_cast<const uint8_t*>(items.data() + items.size()),
             host + (o_items - L.o_desc));
   DTB_CUDA(ctx, cudaMemcpyAsync(sc + L.o_desc, host, hbytes, cudaMemcpyHostToDevice, s->s_in));
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_in1, s->s_in));
   DTB_CUDA(ctx, cudaEventRecord(ws.ev_in, s->s_in));
   DTB_CUDA(ctx, cudaStreamWaitEvent(st, ws.ev_in, 0));
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_run0, st));
   const dtb_status qs = reset_queue(ctx, sc, L, st);
   if (qs != DTB_OK) return qs;
   const ImgDesc* ddesc = reinterpret_cast<const ImgDesc*>(sc + L.o_desc);
@@ -453,7 +514,7 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
     stall_ns = ctx->inject_stall_ns;
     ctx->inject_stall_ns = 0;
   }
-  Queue q = make_queue(sc, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS);
+  Queue q = make_queue(sc, L, stall_ns ? stall_ns : DEFAULT_TIMEOUT_NS, &tuning);
   f.hdr = total > 0 ? reinterpret_cast<QueueHdr*>(sc + L.o_hdr) : nullptr;
   f.total = total;
   if (!items.empty()) {
@@ -479,32 +540,39 @@ dtb_status launch_wave(dtb_server s, InFlight& f) {
       ggdt_phantom_pending<<<1, 1, 0, st>>>(q.hdr);
       DTB_CUDA(ctx, cudaGetLastError());
     }
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(resident_workers(ctx, MODE_NS, tuning) / PERSIST_WPC);
-    cfg.blockDim = dim3(PERSIST_WPC * 32);
-    cfg.dynamicSmemBytes = PERSIST_SMEM;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    void* args[4] = {(void*)&ddesc, (void*)&dtm, (void*)&states, (void*)&q};
-    DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->ns_fn[tuning.variant], args));
+    const dtb_status ls = launch_tile_kernel(ctx, MODE_NS, tuning, ddesc, dtm, states, q, st);
+    if (ls != DTB_OK) return ls;
     ggdt_finalize<<<blocks, 128, 0, st>>>(ddesc, dbase, n, total, states, nullptr, nullptr);
     DTB_CUDA(ctx, cudaGetLastError());
   }
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_run1, st));
   DTB_CUDA(ctx, cudaEventRecord(ws.ev_comp, st));
   // Device -> host: each request's map into its output buffer.
   DTB_CUDA(ctx, cudaStreamWaitEvent(s->s_out, ws.ev_comp, 0));
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_out0, s->s_out));
   for (int i = 0; i < n; ++i) {
     const dtb_image& o = wave[i].r.out;
     if (o.width == 0 || o.height == 0) continue;
     DTB_CUDA(ctx, cudaMemcpy2DAsync(o.buffer, o.pitch, jobs[i].dist, jobs[i].dist_pitch, 4 * (size_t)o.width, o.height,
                                     cudaMemcpyDeviceToHost, s->s_out));
   }
+  DTB_CUDA(ctx, cudaEventRecord(ws.t_out1, s->s_out));
   DTB_CUDA(ctx, cudaEventRecord(ws.ev_done, s->s_out));
   return DTB_OK;
+}
+
+// Adds the stream times of an ended wave's phases to the statistics (caller holds mu).
+void add_wave_times(dtb_server s, const InFlight& f) {
+  const WaveSlot& ws = s->slot[f.slot];
+  float a = 0.0f, b = 0.0f, c = 0.0f;
+  if (cudaEventElapsedTime(&a, ws.t_in0, ws.t_in1) != cudaSuccess) a = 0.0f;
+  if (cudaEventElapsedTime(&b, ws.t_run0, ws.t_run1) != cudaSuccess) b = 0.0f;
+  if (cudaEventElapsedTime(&c, ws.t_out0, ws.t_out1) != cudaSuccess) c = 0.0f;
+  cudaGetLastError();
+  s->st.copy_in_ms += a;
+  s->st.kernel_ms += b;
+  s->st.copy_out_ms += c;
+  s->st.host_prep_ms += f.prep_ms;
 }
 
 // Completes the requests of a wave that has ended (or failed to enqueue): a failed new image is dropped, since
@@ -534,6 +602,7 @@ void worker_main(dtb_server s) {
   auto set_busy_from = [&] { s->busy_from = inflight.empty() ? s->wave_no + 1 : inflight.front().no; };
   for (;;) {
     InFlight f;
+    Clock::time_point t_prep;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       if (inflight.empty()) s->cv_sub.wait(lk, [&] { return s->stop || !s->pending.empty(); });
@@ -541,7 +610,15 @@ void worker_main(dtb_server s) {
       if (inflight.size() < 2 && !s->pending.empty() && s->st.submitted != blocked_at) {
         f.no = ++s->wave_no;
         s->busy_from = inflight.empty() ? f.no : inflight.front().no;  // during admission and while f runs
-        f.reqs = admit(s);
+        bool split = false;
+        t_prep = Clock::now();
+        f.reqs = admit(s, &split);
+        if (split) s->st.waves_split += 1;
+        for (const Request& q : f.reqs) {
+          const double w = std::chrono::duration<double, std::milli>(t_prep - q.t_submit).count();
+          s->st.queue_wait_ms += w;
+          s->st.queue_wait_max_ms = std::max(s->st.queue_wait_max_ms, w);
+        }
         if (f.reqs.empty()) {
           set_busy_from();
           s->cv_done.notify_all();  // admission may have completed invalid requests
@@ -564,6 +641,7 @@ void worker_main(dtb_server s) {
         std::lock_guard<std::mutex> ctx_lock(s->ctx->mu);
         ls = launch_wave(s, f);
       }
+      f.prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t_prep).count();
       if (ls != DTB_OK) {
         // Nothing of this wave may still run when its requests complete.
         cudaStreamSynchronize(s->s_in);
@@ -603,6 +681,7 @@ void worker_main(dtb_server s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->st.tile_visits += ds.tile_visits;
     s->st.tiles += old.total;
+    add_wave_times(s, old);
     retire_wave(s, old, status);
     inflight.pop_front();
     set_busy_from();
@@ -617,7 +696,7 @@ void release_server(dtb_server s) {
     if (w.scratch) cudaFree(w.scratch);
     if (w.stage) cudaFree(w.stage);
     if (w.hpin) cudaFreeHost(w.hpin);
-    for (cudaEvent_t e : {w.ev_in, w.ev_comp, w.ev_done})
+    for (cudaEvent_t e : {w.ev_in, w.ev_comp, w.ev_done, w.t_in0, w.t_in1, w.t_run0, w.t_run1, w.t_out0, w.t_out1})
       if (e) cudaEventDestroy(e);
   }
   for (cudaStream_t t : {s->s_in, s->s_run, s->s_out})
@@ -631,7 +710,8 @@ void release_server(dtb_server s) {
 extern "C" {
 
 DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg, dtb_server* out) {
-  if (!ctx || !cfg || !out || cfg->hbm_budget_bytes == 0 || !(cfg->v >= 0.0f) || cfg->max_wave_requests < 0)
+  if (!ctx || !cfg || !out || cfg->hbm_budget_bytes == 0 || !(cfg->v >= 0.0f) || cfg->max_wave_requests < 0 ||
+      cfg->max_wave_tiles > (1u << 26))
     return DTB_ERR_INVALID_ARG;
   *out = nullptr;
   dtb_server s = new (std::nothrow) dtb_server_s();
@@ -650,13 +730,46 @@ DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg
   bool ok = cudaStreamCreateWithFlags(&s->s_in, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&s->s_run, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&s->s_out, cudaStreamNonBlocking) == cudaSuccess;
-  for (WaveSlot& w : s->slot)
+  for (WaveSlot& w : s->slot) {
     ok = ok && cudaEventCreateWithFlags(&w.ev_in, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&w.ev_comp, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&w.ev_done, cudaEventDisableTiming) == cudaSuccess;
+    for (cudaEvent_t* e : {&w.t_in0, &w.t_in1, &w.t_run0, &w.t_run1, &w.t_out0, &w.t_out1})
+      ok = ok && cudaEventCreate(e) == cudaSuccess;
+  }
   if (!ok) {
     release_server(s);
     return DTB_ERR_CUDA;
+  }
+  // Per-wave buffers for the largest wave the limits admit: scratch (run layout for max_reqs images and
+  // max_tiles tiles with every launch variant's workers, plus warm flags, disks and repitch items), staging and
+  // the pinned tables.
+  s->max_reqs = cfg->max_wave_requests > 0 ? cfg->max_wave_requests : SERVE_MAX_WAVE_REQUESTS;
+  s->max_tiles = cfg->max_wave_tiles > 0 ? cfg->max_wave_tiles : SERVE_MAX_WAVE_TILES;
+  s->stage_cap = cfg->wave_stage_bytes > 0 ? (size_t)cfg->wave_stage_bytes : (size_t)SERVE_WAVE_STAGE_BYTES;
+  for (int k = 0; k < NS_VARIANTS; ++k) {
+    LaunchTuning t = ctx->tuning;
+    t.variant = k;
+    t.grid_percent = 100;
+    s->workers = std::max(s->workers, resident_workers(ctx, MODE_NS, t));
+  }
+  s->nb = (uint32_t)ctx->tuning.buckets;
+  const ScratchLayout Lmax = layout_for(s->max_reqs, s->max_tiles, s->workers, false, s->nb);
+  size_t o_warm = 0, o_disks = 0, o_items = 0;
+  const size_t scratch = wave_scratch_bytes(Lmax, s->max_reqs, SERVE_MAX_WAVE_DISKS, 2 * (size_t)s->max_reqs, &o_warm,
+                                            &o_disks, &o_items);
+  for (WaveSlot& w : s->slot) {
+    ok = ok && cudaMalloc(&w.scratch, scratch) == cudaSuccess && cudaMalloc(&w.stage, s->stage_cap) == cudaSuccess &&
+         cudaHostAlloc((void**)&w.hpin, scratch - Lmax.o_desc, cudaHostAllocDefault) == cudaSuccess;
+    if (!ok) break;
+    w.scratch_size = scratch;
+    w.stage_size = s->stage_cap;
+    w.hpin_size = scratch - Lmax.o_desc;
+  }
+  if (!ok) {
+    cudaGetLastError();
+    release_server(s);
+    return DTB_ERR_OUT_OF_MEMORY;
   }
   s->worker = std::thread(worker_main, s);
   *out = s;
@@ -683,6 +796,7 @@ DTB_API dtb_status dtb_serve_submit(dtb_server s, const dtb_serve_request* r, in
     if (!(r->gamma >= 0.0f) || std::isinf(r->gamma)) return DTB_ERR_INVALID_ARG;
   } else {
     if (r->n_disks < 0 || (r->n_disks > 0 && !r->disks)) return DTB_ERR_INVALID_ARG;
+    if ((size_t)r->n_disks > SERVE_MAX_WAVE_DISKS) return DTB_ERR_CAPACITY;
   }
   Request q;
   q.r = *r;

@@ -21,7 +21,7 @@ extern "C" {
 #endif
 
 #define DTB_API __attribute__((visibility("default")))
-#define DTB_ABI_VERSION 1
+#define DTB_ABI_VERSION 2
 
 typedef enum dtb_status {
   DTB_OK = 0,
@@ -93,16 +93,26 @@ DTB_API dtb_status dtb_last_stats(dtb_context ctx, dtb_stats* out);
  * context, and returns their device status. */
 DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
 
-/* Launch tuning of the ns-mode tile kernel (chosen by dtb_plan_autotune, or set by hand).
- * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128; 0 = keep);
+/* Launch tuning and queue policy of the ns-mode tile kernel (chosen by dtb_plan_autotune, or set by hand).
+ * The reference fixes its choices at build time: 64 priority levels from seed distances
+ * (dt/src/task_queue.cuh:23, dt/src/block_priority.cu:71-155) and 4 blocks of one warp per SM
+ * (dt/src/generalised_distance_transform_task.cu:184).  0 keeps a field's current value.
+ * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128);
  * grid_percent: share of the co-resident CTAs launched, 1..100 (fewer workers re-visit fewer tiles on
- * narrow fronts; 0 = 100); host_chunk_kpx: pixels (in units of 1024) per chunk of the pipeline that serves
- * batches in host memory (host-to-device copies, tile runs on two alternating compute lanes and
- * device-to-host copies of successive chunks overlap; 0 = keep, default 16384). */
+ * narrow fronts); host_chunk_kpx: pixels (in units of 1024) per chunk of the pipeline that serves batches in
+ * host memory (host-to-device copies, tile runs on two alternating compute lanes and device-to-host copies of
+ * successive chunks overlap; default 16384); queue_buckets: 1 = one FIFO ring, or 2 / 4 / 8 / 16 rings ordered
+ * by the distance an activation can bring (default 8); bucket_width_pct: width of one bucket in percent of
+ * one tile-width of path cost of the image (32 x its mean edge weight), 1..6400 (default 50);
+ * staging: 1 = a visit stages its own tile, 2 = a warp stages the image box of its next tile while it visits
+ * the current one (double-buffered shared memory; ctas_per_sm 2 or 3 only). */
 typedef struct dtb_tuning {
   int32_t ctas_per_sm;
   int32_t grid_percent;
   int32_t host_chunk_kpx;
+  int32_t queue_buckets;
+  int32_t bucket_width_pct;
+  int32_t staging;
 } dtb_tuning;
 DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t);
 DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t);
@@ -142,16 +152,29 @@ DTB_API dtb_status dtb_gdt_batch(dtb_context ctx, int32_t n, const dtb_image* im
  * (queue reset, seed scan, the cooperative persistent tile kernel, finalize) in a CUDA graph.  The buffers
  * must stay allocated while the plan lives; their contents may change between runs.  dtb_plan_run launches
  * the graph on `stream` and returns; dtb_plan_wait waits for it and returns the device status and counters
- * (flags: reserved, pass 0).  dtb_plan_autotune times the tile-kernel launch variants on
- * this batch (reps runs each), keeps the fastest in the plan and in the context's cache for batches of the
- * same size class, and reports it.  No reference counterpart. */
+ * (flags: reserved, pass 0).  dtb_plan_autotune searches, on this batch (median of reps runs each), the
+ * tile-kernel variant (CTAs per SM, staging), the grid share and the tile-queue policy (FIFO, or 8 / 16
+ * distance-ordered buckets of 1/4, 1/2 or 1 tile-width of path cost): variants x grid shares first, then the
+ * queue policies under the best launch, then the variants again under the best policy.  It keeps the fastest
+ * in the plan and, for batches of the same size class (image count and tile count, each rounded up to a power
+ * of two), in the context and in its autotuner cache file if one is set; and reports it.  dtb_plan_get_tuning
+ * reports the plan's current tuning.  No reference counterpart: the reference fixes these choices
+ * (dt/src/task_queue.cuh:23, dt/src/generalised_distance_transform_task.cu:184). */
 typedef struct dtb_plan_s* dtb_plan;
 DTB_API dtb_status dtb_plan_create(dtb_context ctx, int32_t n, const dtb_image* imgs, const dtb_image* masks,
                                    const dtb_image* dists, const float* gammas, float v, uint32_t flags, dtb_plan* out);
 DTB_API dtb_status dtb_plan_run(dtb_plan plan, void* stream);
 DTB_API dtb_status dtb_plan_wait(dtb_plan plan, void* stream, dtb_stats* stats);
 DTB_API dtb_status dtb_plan_autotune(dtb_plan plan, void* stream, int32_t reps, dtb_tuning* chosen);
+DTB_API dtb_status dtb_plan_get_tuning(dtb_plan plan, dtb_tuning* out);
 DTB_API void dtb_plan_destroy(dtb_plan plan);
+
+/* Autotuner cache file (JSON, {"format": "dtb-autotune-1", "entries": [...]}, one entry per GPU name and size
+ * class): loads this GPU's entries into the context (plans and calls of those size classes start from them)
+ * and makes dtb_plan_autotune write its results there (entries of other GPUs and size classes are kept; the
+ * file is replaced atomically).  A missing file is not an error; NULL or "" turns the cache off.  The
+ * environment variable DTB_AUTOTUNE_CACHE names a cache that dtb_context_create loads. */
+DTB_API dtb_status dtb_context_set_tuning_cache(dtb_context ctx, const char* path);
 
 /* Serving engine: continuous batching of requests on one device.  A worker thread runs waves: each wave
  * admits, in arrival order, the pending requests that fit the device-memory budget (evicting least recently
@@ -159,13 +182,20 @@ DTB_API void dtb_plan_destroy(dtb_plan plan);
  * arrive meanwhile join the next wave.  Images stay resident with their distance maps, so a seed edit
  * warm-starts from the previous map (exact: added seeds only lower distances).  No reference counterpart.
  * Request data (img, mask, out buffers) is host memory owned by the caller and must stay valid until the
- * request's completion has been returned by dtb_serve_poll; the disk list is copied by dtb_serve_submit. */
+ * request's completion has been returned by dtb_serve_poll; the disk list is copied by dtb_serve_submit.
+ * dtb_serve_create allocates everything the engine uses: the resident arena (hbm_budget_bytes) and, for each of
+ * the two waves that can be in flight, its scratch, staging and pinned table buffers, sized by the per-wave
+ * limits of the config; a wave that would exceed a limit is closed and the rest waits for the next wave, so no
+ * allocation and no device-wide synchronisation happens while waves run.  An edit may add at most 65536 disks. */
 #define DTB_REQ_IMAGE 0  /* new image: img (gray / rgb8), mask, gamma; resident under image_id afterwards */
 #define DTB_REQ_EDIT 1   /* seed edit of the resident image image_id: n_disks disks (cx, cy, r) added */
 typedef struct dtb_serve_config {
   uint64_t hbm_budget_bytes;  /* device memory reserved for resident images, masks and maps */
-  int32_t max_wave_requests;  /* at most this many requests per wave (0 = no limit) */
+  int32_t max_wave_requests;  /* at most this many requests per wave (0 = 4096) */
   float v;                    /* value of unreached pixels (>= 0) */
+  uint32_t max_wave_tiles;    /* at most this many 32 x 32 tiles per wave (0 = 2^20); an image alone above it is
+                                 rejected with DTB_ERR_CAPACITY */
+  uint64_t wave_stage_bytes;  /* device staging per wave for new images whose rows need a new pitch (0 = 256 MiB) */
 } dtb_serve_config;
 typedef struct dtb_serve_request {
   int32_t kind;
@@ -185,6 +215,12 @@ typedef struct dtb_serve_completion {
 typedef struct dtb_serve_stats {
   int64_t submitted, completed, failed, waves, evictions, pending, resident_images;
   uint64_t resident_bytes, tiles, tile_visits;
+  /* Where the time of the ended waves went (sums over waves, milliseconds): host preparation of a wave (admission
+   * to the last enqueue), its copies in (first to last, stream time), its tile run (scan or warm start, persistent
+   * kernel, finalize) and its copies out; and the requests' queueing (submit to the start of their wave's
+   * preparation; sum and maximum over requests). */
+  double host_prep_ms, copy_in_ms, kernel_ms, copy_out_ms, queue_wait_ms, queue_wait_max_ms;
+  int64_t waves_split;        /* waves closed by a per-wave limit (tiles, staging, disks) with requests left over */
 } dtb_serve_stats;
 typedef struct dtb_server_s* dtb_server;
 DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg, dtb_server* out);

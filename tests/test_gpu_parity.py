@@ -389,14 +389,95 @@ def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
     plan.close()
 
 
-@pytest.mark.parametrize("ctas,pct", [(3, 100), (4, 50), (2, 25)])
-def test_every_tuning_gives_the_same_map(ctas, pct):
+TUNINGS = [  # (ctas_per_sm, grid_percent, staging, queue_buckets, bucket_width_pct)
+    (3, 100, 1, 8, 50), (4, 50, 1, 8, 50), (2, 25, 1, 8, 50),    # launch shapes, self-staging visits
+    (3, 100, 2, 8, 50), (2, 75, 2, 16, 25),                        # next tile staged ahead
+    (3, 100, 1, 1, 50), (3, 100, 2, 1, 50),                        # FIFO queue
+    (3, 100, 1, 16, 100), (3, 100, 2, 2, 400), (3, 100, 2, 4, 1),  # bucket counts and widths
+]
+
+
+@pytest.mark.parametrize("ctas,pct,staging,buckets,width", TUNINGS)
+def test_every_tuning_gives_the_same_map(ctas, pct, staging, buckets, width):
+    """Launch shape, staging and queue policy change the visit order only: every one gives the oracle's map,
+    on a single image and on a ragged batch (gray and rgb8, seeds in several tiles)."""
     c = dtb.Context(0)
-    c.set_tuning(ctas_per_sm=ctas, grid_percent=pct)
-    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 16384}
+    c.set_tuning(ctas_per_sm=ctas, grid_percent=pct, staging=staging, queue_buckets=buckets, bucket_width_pct=width)
+    assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 16384,
+                              "queue_buckets": buckets, "bucket_width_pct": width, "staging": staging}
     img, mask, gamma = wl.config0(seed=9)
     d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=c)
-    assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), "tuning %d/%d" % (ctas, pct))
+    what = "tuning %s" % ((ctas, pct, staging, buckets, width),)
+    assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), what)
+    batch = wl.config3(seed=31, n=20, smin=48, smax=700)
+    dists = dtb.geodesic_distance_transform_batch([cuda(i) for i, _, _ in batch], [cuda(m) for _, m, _ in batch],
+                                                  [g for _, _, g in batch], ctx=c)
+    for k, ((i, m, g), dk) in enumerate(zip(batch, dists)):
+        assert_images_eq(dk, orc.ggdt_ns(i, m, g), "%s batch image %d" % (what, k))
+    assert c.stats()["device_error"] == 0
+    c.close()
+
+
+def test_invalid_tunings_are_rejected():
+    c = dtb.Context(0)
+    for kw in ({"ctas_per_sm": 4, "staging": 2}, {"ctas_per_sm": 5}, {"queue_buckets": 3}, {"queue_buckets": 32},
+               {"bucket_width_pct": 6401}, {"staging": 3}, {"grid_percent": 101}):
+        with pytest.raises(dtb.DtbError):
+            c.set_tuning(**kw)
+    c.close()
+
+
+def test_autotuner_cache_round_trip(tmp_path):
+    """dtb_plan_autotune writes its choice to the JSON cache; a new context that loads the cache starts plans
+    of the same size class from it."""
+    import json
+    path = tmp_path / "autotune.json"
+    batch = wl.config3(seed=41, n=12, smin=64, smax=400)
+    imgs = [cuda(i) for i, _, _ in batch]
+    masks = [cuda(m) for _, m, _ in batch]
+    gammas = [g for _, _, g in batch]
+    c = dtb.Context(0)
+    c.set_tuning_cache(path)
+    plan = dtb.BatchPlan(imgs, masks, gammas, ctx=c)
+    chosen = plan.autotune(reps=1)
+    plan.run()
+    plan.wait()
+    for k, (i, m, g) in enumerate(batch):
+        assert_images_eq(plan.dists[k], orc.ggdt_ns(i, m, g), "autotuned image %d" % k)
+    plan.close()
+    c.close()
+    doc = json.loads(path.read_text())
+    assert doc["format"] == "dtb-autotune-1" and len(doc["entries"]) == 1
+    e = doc["entries"][0]
+    assert e["gpu"] == torch.cuda.get_device_name(0)
+    assert {k: e[k] for k in chosen if k != "host_chunk_kpx"} == {k: v for k, v in chosen.items() if k != "host_chunk_kpx"}
+    c2 = dtb.Context(0)
+    c2.set_tuning_cache(path)
+    plan2 = dtb.BatchPlan(imgs, masks, gammas, ctx=c2)
+    assert plan2.tuning() == chosen
+    plan2.close()
+    c2.close()
+
+
+def test_staged_ahead_batch_runs_are_bit_identical_under_load():
+    """The staged-ahead kernel under load: a tile popped ahead is claimed only when its visit starts, so an
+    activation that reaches it while it waits must still be covered.  Repeated full-grid runs of a ragged batch,
+    each compared with the first, the first with the oracle."""
+    c = dtb.Context(0)
+    c.set_tuning(ctas_per_sm=3, staging=2, grid_percent=100)
+    batch = wl.config3(seed=23, n=120, smin=64, smax=1536)
+    imgs = [cuda(i) for i, _, _ in batch]
+    masks = [cuda(m) for _, m, _ in batch]
+    gammas = [g for _, _, g in batch]
+    dists = dtb.geodesic_distance_transform_batch(imgs, masks, gammas, ctx=c)
+    for k in range(0, len(batch), 6):
+        img, mask, g = batch[k]
+        assert_images_eq(dists[k], orc.ggdt_ns(img, mask, g), "ahead batch image %d %s" % (k, img.shape))
+    first = torch.cat([d.flatten() for d in dists])
+    for rep in range(30):
+        dtb.geodesic_distance_transform_batch(imgs, masks, gammas, dists=dists, ctx=c)
+        assert torch.equal(torch.cat([d.flatten() for d in dists]), first), rep
+    assert c.stats()["device_error"] == 0
     c.close()
 
 
