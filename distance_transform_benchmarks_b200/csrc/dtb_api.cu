@@ -90,8 +90,14 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     }
     old = __shfl_sync(~0u, old, 0);
     const uint32_t img = old >> ST_IMG_SHIFT;
-    const ImgDesc dd = descs[img];
-    visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws);
+    if constexpr (MODE == MODE_NS) {
+      const ImgDesc dd = descs[img];
+      visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws);
+    } else {
+      // ref-mode reads the descriptor fields where it uses them (read-only, cached) instead of holding a copy
+      // in registers through the visit.
+      visit_tile<MODE>(descs[img], tmaps, img, t, old, sm, parity, sch, ws);
+    }
   }
   flush_stats(ws, q);
 }
@@ -472,7 +478,9 @@ dtb_status launch_tile_kernel(dtb_context ctx, int mode, const LaunchTuning& t, 
   cfg.numAttrs = 1;
   Queue qa = q;
   void* args[4] = {(void*)&descs, (void*)&tmaps, (void*)&states, (void*)&qa};
-  const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant] : (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
+  const void* fn = mode == MODE_NS ? ctx->ns_fn[t.variant]
+                   : mode == MODE_REF ? (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, REF_CTAS>
+                                      : (const void*)ggdt_persistent<MODE_REF_NOFMA, PERSIST_WPC, REF_CTAS>;
   DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, fn, args));
   return DTB_OK;
 }
@@ -512,8 +520,11 @@ static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayou
     }
     if (mode == MODE_NS)
       ggdt_round<MODE_NS, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
-    else
+    else if (mode == MODE_REF)
       ggdt_round<MODE_REF, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed, total, q);
+    else
+      ggdt_round<MODE_REF_NOFMA, ROUND_WPC><<<blocks, ROUND_WPC * 32, ROUND_SMEM, stream>>>(ddesc, dtm, states, cur, nxt, changed,
+                                                                                           total, q);
     DTB_CUDA(ctx, cudaGetLastError());
     uint32_t err_prog[2] = {0, 0};
     DTB_CUDA(ctx, cudaMemcpyAsync(&hchanged, changed, 4, cudaMemcpyDeviceToHost, stream));
@@ -617,9 +628,11 @@ dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_
   dtb_status s = count_tiles(ctx, jobs, &total);
   if (s != DTB_OK) return s;
   const bool rounds = (flags & DTB_FLAG_ROUNDS) != 0;
-  const int mode = n > 0 ? jobs[0].mode : MODE_NS;
   for (int i = 1; i < n; ++i)
-    if (jobs[i].mode != mode) return fail(ctx, DTB_ERR_INVALID_ARG, "one call covers images of one weight mode");
+    if (jobs[i].mode != jobs[0].mode || jobs[i].ref_fma != jobs[0].ref_fma)
+      return fail(ctx, DTB_ERR_INVALID_ARG, "one call covers images of one weight mode");
+  // Kernel mode: ref-mode calls with left-to-right rounding run their own kernels.
+  const int mode = n == 0 ? MODE_NS : (jobs[0].mode == MODE_REF && !jobs[0].ref_fma) ? MODE_REF_NOFMA : jobs[0].mode;
   LaunchTuning tuning = ctx->tuning;
   auto it = ctx->tuned.find(tuning_key(n, total));
   if (it != ctx->tuned.end()) tuning = it->second;
@@ -758,7 +771,8 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
   ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 4>;
   ctx->ns_fn[3] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 2>;
   ctx->ns_fn[4] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 3>;
-  const void* kref = (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, 2>;
+  const void* kref = (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, REF_CTAS>;
+  const void* kref_nofma = (const void*)ggdt_persistent<MODE_REF_NOFMA, PERSIST_WPC, REF_CTAS>;
   bool ok = true;
   for (int k = 0; k < NS_VARIANTS && ok; ++k) {
     ctx->ns_smem[k] = NS_VARIANT_TABLE[k].ahead ? PERSIST_SMEM_AHEAD : PERSIST_SMEM;
@@ -768,15 +782,22 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
                                                        ctx->ns_smem[k]) == cudaSuccess &&
          ctx->ns_blocks_per_sm[k] >= 1;
   }
+  int ref_bps_nofma = 0;
   ok = ok && cudaFuncSetAttribute(kref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
+       cudaFuncSetAttribute(kref_nofma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) == cudaSuccess &&
        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ref_blocks_per_sm, kref, PERSIST_WPC * 32, PERSIST_SMEM) ==
            cudaSuccess &&
-       ctx->ref_blocks_per_sm >= 1;
+       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ref_bps_nofma, kref_nofma, PERSIST_WPC * 32, PERSIST_SMEM) ==
+           cudaSuccess;
+  ctx->ref_blocks_per_sm = std::min(ctx->ref_blocks_per_sm, ref_bps_nofma);  // one grid size for both roundings
+  ok = ok && ctx->ref_blocks_per_sm >= 1;
   ok = ok &&
        cudaFuncSetAttribute((const void*)ggdt_round<MODE_NS, ROUND_WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)ROUND_SMEM) == cudaSuccess &&
        cudaFuncSetAttribute((const void*)ggdt_round<MODE_REF, ROUND_WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)ROUND_SMEM) == cudaSuccess;
+                            (int)ROUND_SMEM) == cudaSuccess &&
+       cudaFuncSetAttribute((const void*)ggdt_round<MODE_REF_NOFMA, ROUND_WPC>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ROUND_SMEM) == cudaSuccess;
   if (!ok) {
     delete ctx;
     return DTB_ERR_NO_DEVICE;

@@ -35,6 +35,9 @@ constexpr int ST_IMG_SHIFT = 8;
 // Weight modes.
 constexpr int32_t MODE_NS = 0;   // C4, w = sqrt(1 + g2 * dI2), gray or rgb8
 constexpr int32_t MODE_REF = 1;  // C8, D(q) + l_eucl * {1, sqrt2} + l_grad * |dI|, gray (reference weight)
+// Kernel selection only (descriptors keep MODE_REF with ref_fma = 0): ref-mode with left-to-right rounding.  Each
+// rounding has its own tile kernels, so a kernel holds one copy of the ref-mode phase loop.
+constexpr int32_t MODE_REF_NOFMA = 2;
 
 // Device error codes (written once into Queue::error).
 constexpr uint32_t DERR_NONE = 0;

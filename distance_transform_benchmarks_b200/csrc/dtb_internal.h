@@ -22,6 +22,7 @@ constexpr size_t PERSIST_SMEM = PERSIST_WPC * sizeof(WarpSmem) + 128;
 constexpr size_t PERSIST_SMEM_AHEAD = PERSIST_WPC * sizeof(WarpSmemP) + 128;
 constexpr size_t ROUND_SMEM = ROUND_WPC * sizeof(WarpSmem) + 128;
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
+constexpr int REF_CTAS = 3;  // resident CTAs per SM of the ref-mode tile kernels (168 registers)
 // ns-mode tile kernel variants: CTAs (of PERSIST_WPC warps) per SM (at most 255 / 168 / 128 registers for
 // 2 / 3 / 4) and whether a warp stages its next tile ahead (17 KB of shared memory a warp instead of 13 KB, so
 // at most 3 CTAs per SM).

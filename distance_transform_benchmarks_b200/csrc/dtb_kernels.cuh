@@ -140,6 +140,19 @@ __device__ __forceinline__ float* dist_row(const ImgDesc& dd, int y) {
 // line an SM cached earlier can be returned.
 __device__ __forceinline__ float ld_dist(const ImgDesc& dd, int y, int x) { return __ldcg(dist_row(dd, y) + x); }
 
+// Address of column x of row y0 of the distance map, passed through an empty asm that also takes `dep`.  A
+// visit's tile loads and its write-back each take their row addresses from such a base, with different `dep`:
+// the compiler then cannot keep the 32 row addresses of the loads live across the whole visit to reuse them in
+// the write-back (64 registers).
+__device__ __forceinline__ uint8_t* dist_base(const ImgDesc& dd, int y0, int x, uint32_t dep) {
+  uint8_t* p = reinterpret_cast<uint8_t*>(dist_row(dd, y0) + x);
+  asm("" : "+l"(p) : "r"(dep));
+  return p;
+}
+__device__ __forceinline__ float ld_dist_at(const uint8_t* base, int64_t pitch, int y) {
+  return __ldcg(reinterpret_cast<const float*>(base + (int64_t)y * pitch));
+}
+
 // Waits for the TMA transactions on `bar`; its phase parity is bit `pmask` of `pbits`.  Bounded: after
 // TMA_TIMEOUT_NS the error word is set and the wait goes on for as long again, to give a slow copy the chance
 // to land before the warp leaves; after that the wait gives up, and a copy may then still be pending.  The
@@ -297,8 +310,9 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Tile distances in column layout.
   float d[TILE];
   if (!first) {
+    const uint8_t* lb = dist_base(dd, y0, x0 + lane, 0u);
 #pragma unroll
-    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist_at(lb, dd.dist_pitch, y) : INF;
   }
 
   if (!tma_wait(vb.bar, *vb.pbits, vb.pmask, sch.q, tile)) return;
@@ -504,9 +518,10 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // Write back (column layout: each row is one coalesced 128-byte store).
   if (any || first) {
     if (lane < vw) {
+      uint8_t* wb = dist_base(dd, y0, x0 + lane, nph);
 #pragma unroll 4
       for (int y = 0; y < TILE; ++y)
-        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = B[y * W_STRIDE + lane];
+        if (y < vh) *reinterpret_cast<float*>(wb + (int64_t)y * dd.dist_pitch) = B[y * W_STRIDE + lane];
     }
   }
   __threadfence();  // release: distances before activations and before the VISITED bit
@@ -528,7 +543,14 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 // are re-activated when a border pixel facing them decreased, as in dt_block_passes.cuh:50-63, and on
 // visits that applied seeds.
 // ------------------------------------------------------------------------------------------------------
-constexpr int PIMG_STRIDE = 36;  // padded image copy: 34 rows x 36 bytes (odd word stride)
+constexpr int PIMG_STRIDE = 36;  // padded image copies: 34 lines x 36 bytes (9 words a line, odd word stride)
+
+// Pixel at position pos (-1..32) of an image line packed 4 per word (byte (pos + 1) & 3 of word (pos + 1) >> 2)
+// as a float.  pos is a constant after unrolling, so this is one bit-field extract and one conversion.
+__device__ __forceinline__ float line_px(const uint32_t (&w)[9], int pos) {
+  const int i = pos + 1;
+  return (float)((w[i >> 2] >> ((i & 3) * 8)) & 0xFFu);
+}
 
 template <bool FMA>
 __device__ __forceinline__ float ref_min3(float cur, float da, float db, float dc, float le, float lg, float sq2,
@@ -561,13 +583,15 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   stage_tile(vb, tm_img, tm_mask, false, seed, x0, y0);
 
   // Neighbour k = lane (0..7): (dx, dy) = L, R, T, B, TL, TR, BL, BR.
-  const int ndx[8] = {-1, 1, 0, 0, -1, 1, -1, 1};
-  const int ndy[8] = {0, 0, -1, 1, -1, -1, 1, 1};
+  // Offsets of neighbour k = lane, the tables {-1,1,0,0,-1,1,-1,1} and {0,0,-1,1,-1,-1,1,1} as bit masks (an
+  // array indexed by the lane would live in local memory).
+  const int ndx_l = (0xF3u >> lane) & 1u ? ((0xA2u >> lane) & 1u ? 1 : -1) : 0;
+  const int ndy_l = (0xFCu >> lane) & 1u ? ((0xC8u >> lane) & 1u ? 1 : -1) : 0;
   uint32_t nvis, nexist;
   {
     bool vis = false, ex = false;
     if (lane < 8) {
-      const int nx = tx + ndx[lane], ny = ty + ndy[lane];
+      const int nx = tx + ndx_l, ny = ty + ndy_l;
       ex = nx >= 0 && ny >= 0 && nx < dd.tiles_x && ny < dd.tiles_y;
       if (ex) vis = (ld_volatile(&sch.states[dd.tile_base + (uint32_t)(ny * dd.tiles_x + nx)]) & ST_VISITED) != 0;
     }
@@ -601,17 +625,23 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
 
   float d[TILE];
   if (!first) {
+    const uint8_t* lb = dist_base(dd, y0, x0 + lane, 0u);
 #pragma unroll
-    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist(dd, y0 + y, x0 + lane) : INF;
+    for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist_at(lb, dd.dist_pitch, y) : INF;
   }
 
   if (!tma_wait(&sm.bar, parity, 1u, sch.q, tile)) return;
 
-  // Padded copy of the image box: pimg[r * 36 + c + 1] = pixel (tile column c, box row r), c = -1..32.
-  uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.Wh + 96);  // 34 * 36 = 1224 bytes after the halo rows
+  // Padded copies of the image box, one line per tile row and one per tile column (position -1..32 at byte
+  // pos + 1): pimg line r = box row r (tile row r - 1), pimgT line c = tile column c - 1.  In either layout
+  // lane l needs lines l, l + 1, l + 2 (its own line and the two beside it) of one of them.
+  uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.Wh + 96);    // 34 * 36 = 1224 bytes after the halo rows
+  uint8_t* pimgT = reinterpret_cast<uint8_t*>(sm.Wh + 416);  // 1224 bytes after pimg
   for (int i = lane; i < IMG_BOX_ROWS * PIMG_STRIDE; i += 32) {
     const int r = i / PIMG_STRIDE, c = i % PIMG_STRIDE;
-    pimg[i] = (c < TILE + 2) ? sm.img[r * IMG_BOX_GRAY + 15 + c] : 0;
+    const uint8_t px = (c < TILE + 2) ? sm.img[r * IMG_BOX_GRAY + 15 + c] : 0;
+    pimg[i] = px;
+    if (c < TILE + 2) pimgT[c * PIMG_STRIDE + r] = px;
   }
 
   if (first) {
@@ -630,12 +660,16 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   // Tile values live in T (column-layout transposes) = sm.img region after staging is consumed:
   // the image is needed through pimg only from here on.
   float* T = reinterpret_cast<float*>(sm.img);  // 32 x 33 floats = 4224 bytes <= 4352
-  // Initial border values for the change test.
-  const float it0 = d[0], ib0 = d[TILE - 1];
+  // Initial border values for the change test, kept in shared memory through the phases (registers are the
+  // scarce resource there): top, bottom, left, right at border0[32 * side + lane].
+  float* border0 = sm.Wv + 352;  // after the halo columns
+  border0[lane] = d[0];
+  border0[32 + lane] = d[TILE - 1];
 #pragma unroll
   for (int y = 0; y < TILE; ++y) T[y * S_STRIDE + lane] = d[y];
   __syncwarp();
-  const float il0 = T[lane * S_STRIDE], ir0 = T[lane * S_STRIDE + TILE - 1];
+  border0[64 + lane] = T[lane * S_STRIDE];
+  border0[96 + lane] = T[lane * S_STRIDE + TILE - 1];
   __syncwarp();
 
   auto P = [&](int r, int c) -> float {  // pixel at tile (c, r) as float, r, c in [-1, 32]
@@ -677,94 +711,66 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   bool col = true;
   for (;;) {
     bool ch = false;
-    // The forward and the backward chain of the phase are interleaved (two independent dependency chains per
-    // warp); every step is the same single-edge relaxation as in the reference passes, so the order does not
-    // change the fixpoint.
-    if (col) {
-      // Column phase (lane = x): forward over y with predecessors (x-1..x+1, y-1), backward with (x-1..x+1, y+1).
-      const int x = lane;
-      const bool xin = lane < vw;
+    // One code path for both layouts.  Column phase (lane = x, position k = y): forward over y from the three
+    // predecessors (x-1..x+1, y-1), backward from (x-1..x+1, y+1).  Row phase (lane = y, k = x): forward over x
+    // from (x-1, y-1..y+1), backward from (x+1, y-1..y+1).  Lanes l-1 / l+1 hold the diagonal predecessors (by
+    // shuffle); the edge lanes take them from the halo beside the tile (`side_lo` / `side_hi`), and position
+    // -1 / 32 from the halo across the chain (`lo` / `hi`).  The lane's image lines (its own and the two beside
+    // it) are loaded once per phase.  The forward and the backward chain are interleaved (two independent
+    // dependency chains per warp); every step is the same single-edge relaxation as in the reference passes,
+    // so the order does not change the fixpoint.
+    const float* lo = col ? ht : hl;
+    const float* hi = col ? hb : hr;
+    const float* side_lo = col ? hl : ht;
+    const float* side_hi = col ? hr : hb;
+    const bool lane_in = lane < (col ? vw : vh);
+    const int kmax = col ? vh : vw;
+    uint32_t L0[9], L1[9], L2[9];
+    {
+      const uint32_t* w = reinterpret_cast<const uint32_t*>((col ? pimgT : pimg) + lane * PIMG_STRIDE);
 #pragma unroll
-      for (int k = 0; k < TILE; ++k) {
-        {
-          const int y = k;
-          float pa, pb, pc;
-          if (y == 0) { pa = ht[x]; pb = ht[x + 1]; pc = ht[x + 2]; }
-          else {
-            pb = d[y - 1];
-            pa = __shfl_up_sync(~0u, pb, 1);
-            pc = __shfl_down_sync(~0u, pb, 1);
-            if (lane == 0) pa = hl[y];
-            if (lane == TILE - 1) pc = hr[y];
-          }
-          const float c = P(y, x);
-          const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y - 1, x)),
-                                         absd(c, P(y - 1, x + 1)), true, true);
-          const bool upd = xin && y < vh && nd < d[y];
-          ch |= upd;
-          d[y] = upd ? nd : d[y];
-        }
-        {
-          const int y = TILE - 1 - k;
-          float pa, pb, pc;
-          if (y == TILE - 1) { pa = hb[x]; pb = hb[x + 1]; pc = hb[x + 2]; }
-          else {
-            pb = d[y + 1];
-            pa = __shfl_up_sync(~0u, pb, 1);
-            pc = __shfl_down_sync(~0u, pb, 1);
-            if (lane == 0) pa = hl[y + 2];
-            if (lane == TILE - 1) pc = hr[y + 2];
-          }
-          const float c = P(y, x);
-          const float nd = ref_min3<FMA>(d[y], pa, pb, pc, le, lg, sq2, absd(c, P(y + 1, x - 1)), absd(c, P(y + 1, x)),
-                                         absd(c, P(y + 1, x + 1)), true, true);
-          const bool upd = xin && y < vh && nd < d[y];
-          ch |= upd;
-          d[y] = upd ? nd : d[y];
-        }
+      for (int j = 0; j < 9; ++j) {
+        L0[j] = w[j];
+        L1[j] = w[9 + j];
+        L2[j] = w[18 + j];
       }
-    } else {
-      // Row phase (lane = y): forward over x with predecessors (x-1, y-1..y+1), backward with (x+1, y-1..y+1).
-      const int y = lane;
-      const bool yin = lane < vh;
+    }
 #pragma unroll
-      for (int k = 0; k < TILE; ++k) {
-        {
-          const int x = k;
-          float pa, pb, pc;
-          if (x == 0) { pa = hl[y]; pb = hl[y + 1]; pc = hl[y + 2]; }
-          else {
-            pb = d[x - 1];
-            pa = __shfl_up_sync(~0u, pb, 1);
-            pc = __shfl_down_sync(~0u, pb, 1);
-            if (lane == 0) pa = ht[x];
-            if (lane == TILE - 1) pc = hb[x];
-          }
-          const float c = P(y, x);
-          const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x - 1)), absd(c, P(y, x - 1)),
-                                         absd(c, P(y + 1, x - 1)), true, true);
-          const bool upd = yin && x < vw && nd < d[x];
-          ch |= upd;
-          d[x] = upd ? nd : d[x];
+    for (int k = 0; k < TILE; ++k) {
+      {
+        float pa, pb, pc;
+        if (k == 0) { pa = lo[lane]; pb = lo[lane + 1]; pc = lo[lane + 2]; }
+        else {
+          pb = d[k - 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = side_lo[k];
+          if (lane == TILE - 1) pc = side_hi[k];
         }
-        {
-          const int x = TILE - 1 - k;
-          float pa, pb, pc;
-          if (x == TILE - 1) { pa = hr[y]; pb = hr[y + 1]; pc = hr[y + 2]; }
-          else {
-            pb = d[x + 1];
-            pa = __shfl_up_sync(~0u, pb, 1);
-            pc = __shfl_down_sync(~0u, pb, 1);
-            if (lane == 0) pa = ht[x + 2];
-            if (lane == TILE - 1) pc = hb[x + 2];
-          }
-          const float c = P(y, x);
-          const float nd = ref_min3<FMA>(d[x], pa, pb, pc, le, lg, sq2, absd(c, P(y - 1, x + 1)), absd(c, P(y, x + 1)),
-                                         absd(c, P(y + 1, x + 1)), true, true);
-          const bool upd = yin && x < vw && nd < d[x];
-          ch |= upd;
-          d[x] = upd ? nd : d[x];
+        const float c = line_px(L1, k);
+        const float nd = ref_min3<FMA>(d[k], pa, pb, pc, le, lg, sq2, absd(c, line_px(L0, k - 1)),
+                                       absd(c, line_px(L1, k - 1)), absd(c, line_px(L2, k - 1)), true, true);
+        const bool upd = lane_in && k < kmax && nd < d[k];
+        ch |= upd;
+        d[k] = upd ? nd : d[k];
+      }
+      {
+        const int j = TILE - 1 - k;
+        float pa, pb, pc;
+        if (j == TILE - 1) { pa = hi[lane]; pb = hi[lane + 1]; pc = hi[lane + 2]; }
+        else {
+          pb = d[j + 1];
+          pa = __shfl_up_sync(~0u, pb, 1);
+          pc = __shfl_down_sync(~0u, pb, 1);
+          if (lane == 0) pa = side_lo[j + 2];
+          if (lane == TILE - 1) pc = side_hi[j + 2];
         }
+        const float c = line_px(L1, j);
+        const float nd = ref_min3<FMA>(d[j], pa, pb, pc, le, lg, sq2, absd(c, line_px(L0, j + 1)),
+                                       absd(c, line_px(L1, j + 1)), absd(c, line_px(L2, j + 1)), true, true);
+        const bool upd = lane_in && j < kmax && nd < d[j];
+        ch |= upd;
+        d[j] = upd ? nd : d[j];
       }
     }
     ch = __any_sync(~0u, ch);
@@ -791,7 +797,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   }
   if (nph >= (uint32_t)PHASE_LIMIT && lane == 0) set_error(sch.q, DERR_PHASE_LIMIT, tile);
 
-  // Border changes -> neighbours (bit k = neighbour k as in ndx/ndy), as the reference activates blocks
+  // Border changes -> neighbours (bit k = neighbour k as in ndx_l / ndy_l), as the reference activates blocks
   // (dt_block_passes.cuh:50-63).  An exact "can this border lower the neighbour's halo" test (as in ns-mode)
   // removed only a tenth of the visits here and cost more than it saved: most re-visits in ref-mode carry
   // last-bit improvements of equally long paths summed in another order, which that test also lets through.
@@ -802,10 +808,10 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
     const bool force = seed;
     const float bt = T[lane], bb = T[(TILE - 1) * S_STRIDE + lane];
     const float bl = T[lane * S_STRIDE], br = T[lane * S_STRIDE + TILE - 1];
-    const uint32_t ct = __ballot_sync(~0u, force || bt != it0);
-    const uint32_t cb = __ballot_sync(~0u, force || bb != ib0);
-    const uint32_t cl = __ballot_sync(~0u, force || bl != il0);
-    const uint32_t cr = __ballot_sync(~0u, force || br != ir0);
+    const uint32_t ct = __ballot_sync(~0u, force || bt != border0[lane]);
+    const uint32_t cb = __ballot_sync(~0u, force || bb != border0[32 + lane]);
+    const uint32_t cl = __ballot_sync(~0u, force || bl != border0[64 + lane]);
+    const uint32_t cr = __ballot_sync(~0u, force || br != border0[96 + lane]);
     act |= cl ? 1u : 0u;
     act |= cr ? 2u : 0u;
     act |= ct ? 4u : 0u;
@@ -829,22 +835,23 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
 
   if (any || first) {
     if (lane < vw) {
+      uint8_t* wb = dist_base(dd, y0, x0 + lane, nph);
 #pragma unroll
       for (int y = 0; y < TILE; ++y)
-        if (y < vh) dist_row(dd, y0 + y)[x0 + lane] = T[y * S_STRIDE + lane];
+        if (y < vh) *reinterpret_cast<float*>(wb + (int64_t)y * dd.dist_pitch) = T[y * S_STRIDE + lane];
     }
   }
   __threadfence();
   __syncwarp();
   const bool want = lane < 8 && ((act >> lane) & 1u);
-  const uint32_t item = want ? dd.tile_base + (uint32_t)((ty + ndy[lane]) * dd.tiles_x + tx + ndx[lane]) : 0u;
+  const uint32_t item = want ? dd.tile_base + (uint32_t)((ty + ndy_l) * dd.tiles_x + tx + ndx_l) : 0u;
   sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), want, item, key, inv_width);
   *nph_out = nph;
   *nact_out = (uint32_t)__popc(act);
 }
 
-// MODE is fixed per kernel instantiation: a launch covers images of one weight mode only, so the
-// register allocation of the ns-mode kernel is not inflated by the ref-mode code.
+// MODE is fixed per kernel instantiation: a launch covers images of one weight mode (and, in ref-mode, one
+// rounding) only, so no kernel's register allocation is inflated by another mode's code.
 template <int MODE, class Sched>
 __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap* tmaps, uint32_t img, uint32_t tile,
                                            uint32_t old_state, WarpSmem& sm, uint32_t& parity, const Sched& sch,
@@ -854,7 +861,7 @@ __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap*
   uint32_t nph, nact;
   if (MODE == MODE_NS)
     visit_ns<false>(dd, tm_img, tm_mask, tile, old_state, visit_bufs(sm, parity), sch, &nph, &nact);
-  else if (dd.ref_fma)
+  else if (MODE == MODE_REF)
     visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
   else
     visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);

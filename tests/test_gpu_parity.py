@@ -433,8 +433,8 @@ def test_autotuner_cache_round_trip(tmp_path):
     import json
     path = tmp_path / "autotune.json"
     batch = wl.config3(seed=41, n=12, smin=64, smax=400)
-    imgs = [cuda(i) for i, _, _ in batch]
-    masks = [cuda(m) for _, m, _ in batch]
+    imgs = [dtb.pitched_from(i) for i, _, _ in batch]  # plans take TMA-aligned device rows
+    masks = [dtb.pitched_from(m) for _, m, _ in batch]
     gammas = [g for _, _, g in batch]
     c = dtb.Context(0)
     c.set_tuning_cache(path)
