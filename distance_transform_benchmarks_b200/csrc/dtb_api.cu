@@ -506,6 +506,9 @@ static dtb_status run_rounds(dtb_context ctx, uint8_t* dbase, const ScratchLayou
   DTB_CUDA(ctx, cudaMemsetAsync(act0, 0, 2ull * total, stream));
   ggdt_scan<<<scan_blocks, 128, 0, stream>>>(ddesc, dtile_base, L.n, total, states, q, act0, 0);
   DTB_CUDA(ctx, cudaGetLastError());
+  // ref-mode: the first round visits every tile, as the reference's blocks variant does (all blocks active,
+  // dt/src/generalised_distance_transform_blocks.cu:149-151), so per-tile round counters count the same rounds.
+  if (mode != MODE_NS) DTB_CUDA(ctx, cudaMemsetAsync(act0, 1, total, stream));
   uint8_t* cur = act0;
   uint8_t* nxt = act1;
   uint32_t hchanged = 1;

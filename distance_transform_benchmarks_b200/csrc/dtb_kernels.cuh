@@ -244,6 +244,21 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
   return __funnelshift_r(wp[0], wp[1], (off & 3) * 8) & 0xFFFFFFu;
 }
 
+// A lane's row of 32 floats of a W_STRIDE buffer (16-byte aligned), as 8 vector loads / stores.
+__device__ __forceinline__ void load_row(float (&d)[TILE], const float* row) {
+  const float4* p = reinterpret_cast<const float4*>(row);
+#pragma unroll
+  for (int j = 0; j < TILE / 4; ++j) {
+    const float4 v4 = p[j];
+    d[4 * j] = v4.x; d[4 * j + 1] = v4.y; d[4 * j + 2] = v4.z; d[4 * j + 3] = v4.w;
+  }
+}
+__device__ __forceinline__ void store_row(float* row, const float (&d)[TILE]) {
+  float4* p = reinterpret_cast<float4*>(row);
+#pragma unroll
+  for (int j = 0; j < TILE / 4; ++j) p[j] = make_float4(d[4 * j], d[4 * j + 1], d[4 * j + 2], d[4 * j + 3]);
+}
+
 // ------------------------------------------------------------------------------------------------------
 // ns-mode visit (C4, w = sqrt(1 + g2 * dI2)), gray or rgb8.
 //
@@ -256,10 +271,10 @@ __device__ __forceinline__ uint32_t box_pix(const uint8_t* box, bool rgb, int r,
 // re-activated only if some border pixel plus its edge weight is below the halo value it was compared with.
 //
 // One code path serves both layouts (the phase loop is small enough to stay in the instruction cache): the
-// weights live in shared memory as Wh / Wv (stride 33, conflict-free for a lane-per-row and a lane-per-column
-// read alike) and are loaded into registers for the phase's layout; the tile changes layout through B.
-// Element k of lane l is at [k * 33 + l] of the row-major arrays in the column layout, at [l * 33 + k] in the
-// row layout (immediate offsets from one base pointer per lane).
+// weights live in shared memory as Wh / Wv (stride 36: scalar lane-per-column reads and 16-byte lane-per-row
+// reads are conflict-free) and are loaded into registers for the phase's layout; the tile changes layout through
+// B.  Element k of lane l is at [k * 36 + l] of the row-major arrays in the column layout (scalar loads), at
+// [l * 36 + k] in the row layout (16-byte vectors).
 // Returns the number of phases and activations through *nph / *nact.
 // ------------------------------------------------------------------------------------------------------
 template <bool PRESTAGED, class Sched>
@@ -438,9 +453,7 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
                                            __fadd_rn(bot, vb.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
     if (hside && !vside) {
       col = false;
-      const float* qb = B + lane * W_STRIDE;
-#pragma unroll
-      for (int k = 0; k < TILE; ++k) d[k] = qb[k];
+      load_row(d, B + lane * W_STRIDE);
     }
     __syncwarp();
   }
@@ -448,20 +461,22 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   uint32_t nph = 0;
   for (;;) {
     float wc[TILE + 1], wx[TILE];
-    if (col) {  // element k of lane x: [k * 33 + x]
+    if (col) {  // element k of lane x: [k * 36 + x]
       const float* pc = vb.Wv + lane;
       const float* px = vb.Wh + lane;
 #pragma unroll
       for (int k = 0; k <= TILE; ++k) wc[k] = pc[k * W_STRIDE];
 #pragma unroll
       for (int k = 0; k < TILE; ++k) wx[k] = px[k * W_STRIDE];
-    } else {    // element k of lane y: [y * 33 + k]
-      const float* pc = vb.Wh + lane * W_STRIDE;
-      const float* px = vb.Wv + lane * W_STRIDE;
+    } else {    // element k of lane y: [y * 36 + k], as 16-byte vectors
+      const float4* pc = reinterpret_cast<const float4*>(vb.Wh + lane * W_STRIDE);
 #pragma unroll
-      for (int k = 0; k <= TILE; ++k) wc[k] = pc[k];
-#pragma unroll
-      for (int k = 0; k < TILE; ++k) wx[k] = px[k];
+      for (int j = 0; j < 8; ++j) {
+        const float4 v4 = pc[j];
+        wc[4 * j] = v4.x; wc[4 * j + 1] = v4.y; wc[4 * j + 2] = v4.z; wc[4 * j + 3] = v4.w;
+      }
+      wc[TILE] = pc[8].x;
+      load_row(wx, vb.Wv + lane * W_STRIDE);
     }
     bool ch = sweep_phase(d, wc, wx, col ? top : lft, col ? bot : rgt);
     ch = __any_sync(~0u, ch);
@@ -476,13 +491,9 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
       for (int k = 0; k < TILE; ++k) pb[k * W_STRIDE] = d[k];
       __syncwarp();
       if (stop) break;
-      const float* qb = B + lane * W_STRIDE;
-#pragma unroll
-      for (int k = 0; k < TILE; ++k) d[k] = qb[k];
+      load_row(d, B + lane * W_STRIDE);
     } else {
-      float* pb = B + lane * W_STRIDE;
-#pragma unroll
-      for (int k = 0; k < TILE; ++k) pb[k] = d[k];
+      store_row(B + lane * W_STRIDE, d);
       __syncwarp();
       if (stop) break;
       const float* qb = B + lane;

@@ -129,8 +129,9 @@ DTB_API dtb_status dtb_gdt_ref(dtb_context ctx, const dtb_image* img, const dtb_
  * (generalised_distance_transform.hpp:13-15, _blocks.cu:114-165): ref-mode GGDT by host-driven rounds over
  * active 32x32 tiles (DTB_FLAG_ROUNDS is implied).  rounds_per_tile, if not NULL, points to
  * ceil(width/32) * ceil(height/32) int32 counters, tile (bx, by) at index by * ceil(width/32) + bx, in host or
- * device memory; each is incremented once per round in which its tile was visited (the first round visits
- * the tiles holding seeds, where the reference's first round visits every tile).  Same map as dtb_gdt_ref. */
+ * device memory; each is incremented once per round in which its tile was visited.  As in the reference, the
+ * first round visits every tile and a tile runs again in a later round when a neighbour's border changed.
+ * Same map as dtb_gdt_ref. */
 DTB_API dtb_status dtb_gdt_ref_blocks(dtb_context ctx, const dtb_image* img, const dtb_image* mask, const dtb_image* dist,
                                       float lambda, float v, int32_t* rounds_per_tile, uint32_t flags, void* stream);
 

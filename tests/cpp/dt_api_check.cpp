@@ -135,9 +135,12 @@ namespace
           any_seed = true;
           break;
         }
-    if (any_seed)
-      for (int t = 0; t < tiles; ++t)
-        CHECK(rounds[t] >= 1, "%s: tile %d never visited", c.name.c_str(), t);
+    // As in the reference's blocks variant, the first round visits every tile; without seeds nothing changes, so
+    // every tile runs in exactly that one round.
+    for (int t = 0; t < tiles; ++t) {
+      CHECK(rounds[t] >= 1, "%s: tile %d never visited", c.name.c_str(), t);
+      if (!any_seed) CHECK(rounds[t] == 1, "%s: tile %d counted %d rounds without seeds", c.name.c_str(), t, rounds[t]);
+    }
     write_map(dir + "/" + c.name + ".out", d1);
   }
 

@@ -101,6 +101,9 @@ def test_cpp_layer_on_gpu(tmp_path):
     mask[115, 125] = 1
     _write_case(d, lines, "random_ref", "ref", img, mask, 0.3)
     expect["random_ref"] = orc.ggdt_ref(img, mask, 0.3, fma=True)
+    # no seeds: every tile runs in exactly the first blocks round (the reference's first round visits them all)
+    _write_case(d, lines, "noseed_ref", "ref", img[:100, :140], np.zeros((100, 140), np.uint8), 0.5)
+    expect["noseed_ref"] = orc.ggdt_ref(img[:100, :140], np.zeros((100, 140), np.uint8), 0.5, fma=True)
     g, m, gamma = wl.config0()
     _write_case(d, lines, "blobs_c4", "c4", g, m, gamma)
     expect["blobs_c4"] = orc.ggdt_ns(g, m, gamma)
