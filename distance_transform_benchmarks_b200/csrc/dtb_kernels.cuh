@@ -441,16 +441,21 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   // never reads the left / right halo, so a tile reached only from the side would spend its first column
   // phase without any effect.
   bool col = true;
+  // hside / vside: whether the left / right (top / bottom) halo can lower the tile as it stands.  A phase that
+  // changes nothing proves every internal edge and its own axis's halo edges satisfied; if the first phase
+  // changes nothing and the other axis's halo could not lower the unchanged tile, the tile is at its fixpoint
+  // and the visit ends after that one phase (a false-positive activation costs one phase, not two).
+  bool hside, vside;
   {
     float* pb = B + lane;
 #pragma unroll
     for (int k = 0; k < TILE; ++k) pb[k * W_STRIDE] = d[k];
     __syncwarp();
     const float dl = B[lane * W_STRIDE], dr = B[lane * W_STRIDE + TILE - 1];
-    const bool hside = __any_sync(~0u, __fadd_rn(lft, vb.Wh[lane * W_STRIDE]) < dl ||
-                                           __fadd_rn(rgt, vb.Wh[lane * W_STRIDE + TILE]) < dr);
-    const bool vside = __any_sync(~0u, __fadd_rn(top, vb.Wv[lane]) < d[0] ||
-                                           __fadd_rn(bot, vb.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
+    hside = __any_sync(~0u, __fadd_rn(lft, vb.Wh[lane * W_STRIDE]) < dl ||
+                                 __fadd_rn(rgt, vb.Wh[lane * W_STRIDE + TILE]) < dr);
+    vside = __any_sync(~0u, __fadd_rn(top, vb.Wv[lane]) < d[0] ||
+                                 __fadd_rn(bot, vb.Wv[TILE * W_STRIDE + lane]) < d[TILE - 1]);
     if (hside && !vside) {
       col = false;
       load_row(d, B + lane * W_STRIDE);
@@ -484,7 +489,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
     ran_col |= col;
     ran_row |= !col;
     ++nph;
-    const bool stop = (!ch && ran_col && ran_row) || nph >= (uint32_t)PHASE_LIMIT;
+    const bool stop = (!ch && ((ran_col && ran_row) || (nph == 1 && !(col ? hside : vside)))) ||
+                      nph >= (uint32_t)PHASE_LIMIT;
     if (col) {
       float* pb = B + lane;
 #pragma unroll
