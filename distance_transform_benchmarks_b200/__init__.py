@@ -331,8 +331,9 @@ def geodesic_distance_transform_batch(imgs, masks, gammas, v=DEFAULT_V, dists=No
 
 
 def imread(path, channels=1):
-    """dt::imread (reference dt/src/imread.cpp): an 8-bit PNG / PGM / PPM file as a uint8 array, [H, W] for
-    channels=1 (the file must be gray), [H, W, 3] for channels=3 (rgb or palette)."""
+    """dt::imread (reference dt/src/imread.cpp): an 8-bit PNG / PGM / PPM / JPEG file as a uint8 array, [H, W] for
+    channels=1 (the file must be gray), [H, W, 3] for channels=3 (rgb, palette or colour JPEG).  Gray JPEG samples
+    are identical to those of stb_image, the reference's decoder."""
     im = DtbImage()
     st = lib().dtb_image_read(str(path).encode(), int(channels), ctypes.byref(im))
     if st != 0:

@@ -64,7 +64,8 @@ def _deps(*names):
 
 def build_dtb(force=False, verbose=False, ptxas_verbose=False):
     out = os.path.join(HERE, "libdtb.so")
-    srcs = ["dtb_api.cu", "dtb_plan.cu", "dtb_host_pipeline.cu", "dtb_serve.cu", "dtb_noalloc.cu", "dtb_io.cpp"]
+    srcs = ["dtb_api.cu", "dtb_plan.cu", "dtb_host_pipeline.cu", "dtb_serve.cu", "dtb_noalloc.cu", "dtb_io.cpp",
+            "dtb_jpeg.cpp"]
     srcs = [s for s in srcs if os.path.exists(os.path.join(CSRC, s))]
     if force or _stale(out, _deps(*srcs)):
         cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC, "-shared", "-o", out]

@@ -2,7 +2,7 @@
 
     python -m distance_transform_benchmarks_b200.cli input lambda output [mask]
 
-reads a gray 8-bit image (PNG / PGM), seeds it at the non-zero pixels of `mask` (default: the centre pixel),
+reads a gray 8-bit image (PNG / PGM / JPEG), seeds it at the non-zero pixels of `mask` (default: the centre pixel),
 runs the reference-weight transform (C8, lambda blend) on the GPU and writes the map normalised to 0..255 as a
 gray image (the reference colours it with the inferno map, which is not part of this library).  With
 ``--c4 GAMMA`` it runs the C4 geodesic weight sqrt(1 + gamma^2 |dI|^2) instead (gray or, with ``--rgb``, rgb8

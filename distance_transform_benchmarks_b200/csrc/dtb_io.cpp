@@ -1,5 +1,6 @@
 // dtb_io.cpp -- image files for the C ABI (dtb_image_read / dtb_image_write), the reference's dt::imread /
-// dt::imsave (dt/src/imread.cpp, dt/src/imsave.cpp, which use stb_image): 8-bit PNG and binary PGM / PPM.
+// dt::imsave (dt/src/imread.cpp, dt/src/imsave.cpp, which use stb_image): 8-bit PNG and binary PGM / PPM here,
+// JPEG (read only) in dtb_jpeg.cpp.
 //
 // PNG follows the published format (ISO/IEC 15948): chunks with CRC-32, one zlib stream over the IDAT chunks,
 // per-row filter types 0-4 (None, Sub, Up, Average, Paeth).  Read: colour types 0 (gray), 2 (rgb), 3 (palette,
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "dtb.h"
+#include "dtb_imgfile.h"
 
 namespace {
 
@@ -53,11 +55,7 @@ void put_be32(std::vector<uint8_t>& v, uint32_t x) {
   v.push_back((uint8_t)x);
 }
 
-// Host pixels: rows of width * channels bytes (packed).
-struct Pixels {
-  int w = 0, h = 0, channels = 0;
-  std::vector<uint8_t> data;
-};
+using dtb_io::Pixels;
 
 uint8_t paeth(int a, int b, int c) {
   const int p = a + b - c;
@@ -95,7 +93,7 @@ dtb_status decode_png(const std::vector<uint8_t>& f, Pixels& out) {
     pos += 12 + (size_t)len;
   }
   if (w <= 0 || h <= 0 || interlace != 0) return DTB_ERR_INVALID_ARG;
-  if ((uint64_t)w * (uint64_t)h > (1ull << 31)) return DTB_ERR_INVALID_ARG;  // beyond any image the library runs
+  if ((uint64_t)w * (uint64_t)h > dtb_io::kMaxFilePixels) return DTB_ERR_INVALID_ARG;
   int comp;
   switch (ctype) {
     case 0: comp = 1; break;
@@ -215,7 +213,11 @@ static dtb_status image_read(const char* path, int32_t channels, dtb_image* out)
   std::vector<uint8_t> f;
   if (!read_file(path, f)) return DTB_ERR_IO;
   Pixels px;
-  dtb_status s = (f.size() >= 2 && f[0] == 'P') ? decode_pnm(f, px) : decode_png(f, px);
+  dtb_status s;
+  if (f.size() >= 2 && f[0] == 0xFF && f[1] == 0xD8)  // JPEG start-of-image marker
+    s = dtb_io::decode_jpeg(f.data(), f.size(), px);
+  else
+    s = (f.size() >= 2 && f[0] == 'P') ? decode_pnm(f, px) : decode_png(f, px);
   if (s != DTB_OK) return s;
   if (px.channels != channels) return DTB_ERR_INVALID_ARG;  // as the reference: no conversion between kinds
   if ((s = dtb_image_alloc(px.w, px.h, channels, DTB_CPU, out)) != DTB_OK) return s;

@@ -1,6 +1,7 @@
 // dt/imread.hpp -- read an image file into a CPU image, reference dt::imread (dt/include/dt/imread.hpp:7-8,
 // dt/src/imread.cpp): imread<std::uint8_t> wants a one-component (gray) file, imread<rgb8> a three-component
-// one.  Formats: 8-bit PNG and binary PGM / PPM (dtb_image_read); the reference reads any stb_image format.
+// one.  Formats: 8-bit PNG, binary PGM / PPM and JPEG (dtb_image_read; gray JPEG samples identical to stb_image's);
+// the reference reads any stb_image format.
 // Throws std::runtime_error when the file cannot be read, std::invalid_argument when it has the wrong number of
 // components or an unsupported encoding.
 #pragma once
@@ -26,7 +27,7 @@ namespace dt
       throw std::runtime_error(std::string("Error while loading ") + filename);
     if (s == DTB_ERR_INVALID_ARG)
       throw std::invalid_argument(std::string("Input image must have ") + (sizeof(T) == 1 ? "1 component" : "3 components") +
-                                  " of 8 bits (PNG, PGM or PPM): " + filename);
+                                  " of 8 bits (PNG, PGM, PPM or JPEG): " + filename);
     details::check(s, "imread");
     image2d<T> out(file.width, file.height);
     for (int y = 0; y < file.height; ++y)

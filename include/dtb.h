@@ -263,8 +263,10 @@ DTB_API dtb_status dtb_image_free(dtb_image* img);
 
 /* Image files, reference dt::imread / dt::imsave (dt/include/dt/imread.hpp:7-8, imsave.hpp:13-43; the reference
  * reads any stb_image format and writes PNG).  Formats: PNG (read: gray, gray + alpha, rgb, rgba, palette at 8 bits
- * per sample, gray and palette also at 1 / 2 / 4, not interlaced; write: 8-bit gray or rgb) and binary PGM / PPM, chosen by the file name (.png, .pgm, .ppm) on write
- * and by the contents on read.  dtb_image_read: `channels` 1 (gray) or 3 (rgb8) must match the file's
+ * per sample, gray and palette also at 1 / 2 / 4, not interlaced; write: 8-bit gray or rgb), binary PGM / PPM, and
+ * JPEG on read (baseline, extended and progressive Huffman frames of 8-bit samples, 1 or 3 components, restart
+ * intervals; gray samples identical to stb_image's, the decoder the reference's benchmark inputs go through),
+ * chosen by the file name (.png, .pgm, .ppm) on write and by the contents on read.  dtb_image_read: `channels` 1 (gray) or 3 (rgb8) must match the file's
  * components, as the reference requires one component for imread<uint8_t>; the pixels go into new host memory
  * (free with dtb_image_free).  dtb_image_write: a host image of elem_size 1 or 3. */
 DTB_API dtb_status dtb_image_read(const char* path, int32_t channels, dtb_image* out);

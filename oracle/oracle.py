@@ -38,14 +38,41 @@ REF_TESTS = ("image_view", "image2d", "c4", "rgb8", "io", "transfert", "distance
 
 def build_ref(ref_root, force=False):
     """Builds, from the reference source tree at `ref_root`, into _ref/: the reference's tile-pass device
-    functions (libref_passes.so, see ref_passes_driver.cu) and the reference's own unit tests compiled against
-    include/dt and libdtb (test_<name>, see gtest_shim/).  libdtb must be built first.  Returns False if
+    functions (libref_passes.so, see ref_passes_driver.cu), the reference's image decoder (libstb_ref.so, the
+    reference's dt/src/stb_image_implementation.c) and the reference's own unit tests compiled against include/dt
+    and libdtb (test_<name>, see gtest_shim/).  libdtb must be built first.  Returns False if
     `ref_root` is absent."""
     if not os.path.isdir(os.path.join(ref_root, "dt", "src")):
         return False
-    subprocess.run(["make", "-s", "-C", HERE, "ref", "ref-tests", "REF_ROOT=" + ref_root] + (["-B"] if force else []),
-                   check=True)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", "stb-ref", "ref-tests", "REF_ROOT=" + ref_root] +
+                   (["-B"] if force else []), check=True)
     return True
+
+
+STB_REF_PATH = os.path.join(HERE, "_ref", "libstb_ref.so")
+
+
+def stb_ref_available():
+    return os.path.exists(STB_REF_PATH)
+
+
+def stb_ref_load(path, req_comp=0):
+    """The reference's image decoder (stb_image, built by build_ref from the reference's own source) on a file:
+    stbi_load(path, &w, &h, &n, req_comp) as dt::imread calls it (dt/src/imread.cpp:14, req_comp = 0).  Returns
+    (uint8 array [h, w, n'], n) with n' = req_comp or n, or None when stb_image rejects the file."""
+    lib = ctypes.CDLL(STB_REF_PATH)
+    lib.stbi_load.restype = ctypes.POINTER(ctypes.c_uint8)
+    lib.stbi_load.argtypes = [ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.c_int]
+    w, h, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    p = lib.stbi_load(str(path).encode(), ctypes.byref(w), ctypes.byref(h), ctypes.byref(n), int(req_comp))
+    if not p:
+        return None
+    try:
+        ch = req_comp or n.value
+        a = np.ctypeslib.as_array(p, shape=(h.value * w.value * ch,)).reshape(h.value, w.value, ch).copy()
+    finally:
+        lib.stbi_image_free(ctypes.cast(p, ctypes.c_void_p))
+    return a, n.value
 
 
 def ref_test_binary(name):
