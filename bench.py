@@ -378,12 +378,10 @@ def run_configs(ctx, stream):
     return out, maps
 
 
-def run_serve(args, dev):
-    """Serving workload: Poisson arrivals; 60 % new images (sides log-uniform in [256, 4096], gray blobs or rgb8
-    Voronoi, 1-8 seed disks), 40 % seed edits (1-3 disks of radius 3) of a resident image, warm-started from its
-    map.  Latency is measured by the engine from submit to the map being in host memory."""
+def serve_pool():
+    """The serving workload's images: sides log-uniform in [256, 4096], gray blobs or rgb8 Voronoi, 1-8 seed
+    disks, pinned host buffers (an output map per image, shared by its requests)."""
     import math
-    import distance_transform_benchmarks_b200 as dtb
     from distance_transform_benchmarks_b200 import workloads as wl
 
     rng = np.random.default_rng(4)
@@ -395,26 +393,37 @@ def run_serve(args, dev):
         img, mask, g = wl.make_image(("gray" if i % 2 == 0 else "rgb8", w, h, g, 1000 + i))
         out = torch.empty((h, w), dtype=torch.float32).pin_memory()  # shared by the pool image's requests
         pool.append((torch.from_numpy(img).pin_memory(), torch.from_numpy(mask).pin_memory(), g, out))
-    srv = dtb.Server(SERVE_BUDGET, device=dev)
+    return pool
+
+
+def run_serve(args, dev, pool, live=False):
+    """Serving workload: Poisson arrivals; 60 % new images (the pool's), 40 % seed edits (1-3 disks of radius 3)
+    of a resident image, warm-started from its map.  Latency is measured by the engine from submit to the map
+    being in host memory.  live: requests join the tile queue of one running kernel instead of waves (the same
+    request stream, seeded alike)."""
+    import distance_transform_benchmarks_b200 as dtb
+
+    rng = np.random.default_rng(5)
+    srv = dtb.Server(SERVE_BUDGET, device=dev, live=live)
     n = args.serve_requests
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
     kinds = rng.random(n) < 0.6
-    live = []          # (image id, pool index) of images created so far
+    created = []       # image ids created so far
     pool_of = {}
     next_id = 0
 
     def submit(new_image):
         """One request of the mix; returns its pixels."""
         nonlocal next_id
-        if new_image or not live:
+        if new_image or not created:
             p = next_id % SERVE_POOL
             img, mask, g, out = pool[p]
             srv.submit_image(next_id, img, mask, g, out)
-            live.append(next_id)
+            created.append(next_id)
             pool_of[next_id] = p
             next_id += 1
         else:
-            iid = live[int(rng.integers(max(0, len(live) - 256), len(live)))]
+            iid = created[int(rng.integers(max(0, len(created) - 256), len(created)))]
             img, _, _, out = pool[pool_of[iid]]
             hh, ww = img.shape[:2]
             disks = [(int(rng.integers(0, ww)), int(rng.integers(0, hh)), 3) for _ in range(int(rng.integers(1, 4)))]
@@ -443,9 +452,19 @@ def run_serve(args, dev):
 
     def phases(a, b):
         """Where the time of the waves between stats a and b went (per wave: host preparation, copies in, tile
-        run, copies out on their streams; per request: queueing before its wave's preparation)."""
-        w = max(1, b["waves"] - a["waves"])
+        run, copies out on their streams; per request: queueing before its wave's preparation).  Live engine:
+        per request, host clock: publish, publish to its completion word (copy in + tile work), copy out;
+        "waves" counts kernel launches."""
         r = max(1, b["completed"] - a["completed"])
+        if live:
+            return {"launches": int(b["waves"] - a["waves"]),
+                    "host_prep_ms_per_request": (b["host_prep_ms"] - a["host_prep_ms"]) / r,
+                    "in_and_kernel_ms_per_request": (b["kernel_ms"] - a["kernel_ms"]) / r,
+                    "copy_out_ms_per_request": (b["copy_out_ms"] - a["copy_out_ms"]) / r,
+                    "queue_wait_mean_ms": (b["queue_wait_ms"] - a["queue_wait_ms"]) / r,
+                    "queue_wait_max_ms": b["queue_wait_max_ms"],
+                    "tile_visits_per_tile": (b["tile_visits"] - a["tile_visits"]) / max(1, b["tiles"] - a["tiles"])}
+        w = max(1, b["waves"] - a["waves"])
         return {"waves": int(b["waves"] - a["waves"]), "waves_split": int(b["waves_split"] - a["waves_split"]),
                 "host_prep_ms_per_wave": (b["host_prep_ms"] - a["host_prep_ms"]) / w,
                 "copy_in_ms_per_wave": (b["copy_in_ms"] - a["copy_in_ms"]) / w,
@@ -474,7 +493,8 @@ def run_serve(args, dev):
                      "note": "all requests submitted at t=0 (latency includes queueing behind earlier requests)"}
     srv.close()
     lat = np.array(lat)
-    return {"requests": n, "rate_rps": args.serve_rate, "new_fraction": 0.6, "completed": int(st["completed"]),
+    return {"engine": "live admission into one running tile kernel" if live else "waves (two in flight)",
+            "requests": n, "rate_rps": args.serve_rate, "new_fraction": 0.6, "completed": int(st["completed"]),
             "failed": int(st["failed"]), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "throughput_rps": len(lat) / elapsed, "mpx_s": px / 1e6 / elapsed,
             "waves": int(st["waves"]), "requests_per_wave": len(lat) / max(1, st["waves"]),
@@ -713,10 +733,13 @@ def run_ours(args, dist):
     parity.update({"fixpoint_images": len(batch), "fixpoint_violations": viol,
                    "fixpoint_check": "every map of the timed batch: no edge lowers a value and every value is "
                                      "realised (exact greatest-fixpoint characterisation, on the GPU)"})
-    serve = None
+    serve = serve_live = None
     if not args.no_serve and one_gpu:
         himgs = hmasks = hdists = None  # release pinned host memory of the e2e leg
-        serve = run_serve(args, dev)
+        pool = serve_pool()
+        serve = run_serve(args, dev, pool)
+        serve_live = run_serve(args, dev, pool, live=True)
+        pool = None
 
     if dist.rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
@@ -743,6 +766,7 @@ def run_ours(args, dist):
                                "phases_per_visit": stats["phases"] / max(1, stats["tile_visits"])},
                 "gpu_launches": 3 * args.steps,
                 "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "serve": serve,
+                "serve_live": serve_live,
                 "ref_mode": ref_mode, "configs": configs}
         print(json.dumps(line), flush=True)
     plan.close()

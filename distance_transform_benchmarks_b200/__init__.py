@@ -439,13 +439,14 @@ class BatchPlan:
 class Server:
     """dtb_server: continuous batching of new-image and seed-edit requests (see include/dtb.h).  Inputs and the
     output map are host tensors (pinned memory copies fastest); they are kept alive here until the request's
-    completion has been polled."""
+    completion has been polled.  live=True: requests join the tile queue of one persistent kernel that keeps
+    running (live admission) instead of running in waves."""
 
     def __init__(self, hbm_budget_bytes, *, max_wave_requests=0, v=DEFAULT_V, max_wave_tiles=0, wave_stage_bytes=0,
-                 ctx=None, device=0):
+                 live=False, live_idle_us=0, ctx=None, device=0):
         self.ctx = ctx if ctx is not None else default_context(device)
         cfg = DtbServeConfig(int(hbm_budget_bytes), int(max_wave_requests), float(v), int(max_wave_tiles),
-                             int(wave_stage_bytes))
+                             int(wave_stage_bytes), 1 if live else 0, int(live_idle_us))
         self._h = ctypes.c_void_p()
         st = lib().dtb_serve_create(self.ctx.handle, ctypes.byref(cfg), ctypes.byref(self._h))
         if st != 0:

@@ -71,7 +71,8 @@ class DtbTuning(ctypes.Structure):
 
 class DtbServeConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_wave_requests", ctypes.c_int32), ("v", ctypes.c_float),
-                ("max_wave_tiles", ctypes.c_uint32), ("wave_stage_bytes", ctypes.c_uint64)]
+                ("max_wave_tiles", ctypes.c_uint32), ("wave_stage_bytes", ctypes.c_uint64), ("live", ctypes.c_int32),
+                ("live_idle_us", ctypes.c_uint32)]
 
 
 class DtbServeRequest(ctypes.Structure):

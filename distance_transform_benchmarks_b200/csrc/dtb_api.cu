@@ -333,6 +333,36 @@ ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, u
   return L;
 }
 
+dtb_status fill_desc(dtb_context ctx, const Job& j, uint32_t tile_base, int index, ImgDesc* d, CUtensorMap* tm) {
+  d->img = j.img;
+  d->mask = j.mask;
+  d->dist = j.dist;
+  d->img_pitch = j.img_pitch;
+  d->mask_pitch = j.mask_pitch;
+  d->dist_pitch = j.dist_pitch;
+  d->width = j.width;
+  d->height = j.height;
+  d->channels = j.channels;
+  d->tiles_x = j.tiles_x();
+  d->tiles_y = j.tiles_y();
+  d->tile_base = tile_base;
+  d->g2 = j.g2;
+  d->v = j.v;
+  d->l_eucl = j.l_eucl;
+  d->l_grad = j.l_grad;
+  d->mode = j.mode;
+  d->ref_fma = j.ref_fma;
+  if (j.width > 0 && j.height > 0) {
+    const uint32_t bw = j.channels == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY;
+    if (!encode_u8_2d(ctx, &tm[0], j.img, (uint64_t)j.width * j.channels, (uint64_t)j.height, (uint64_t)j.img_pitch, bw,
+                      IMG_BOX_ROWS))
+      return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the image layout", index);
+    if (!encode_u8_2d(ctx, &tm[1], j.mask, (uint64_t)j.width, (uint64_t)j.height, (uint64_t)j.mask_pitch, TILE, TILE))
+      return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the mask layout", index);
+  }
+  return DTB_OK;
+}
+
 dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const ScratchLayout& L, std::vector<uint8_t>& out) {
   const int n = (int)jobs.size();
   out.assign(L.o_act - L.o_desc, 0);
@@ -341,37 +371,10 @@ dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const Scr
   uint32_t* hbase = reinterpret_cast<uint32_t*>(out.data() + (L.o_base - L.o_desc));
   uint32_t base = 0;
   for (int i = 0; i < n; ++i) {
-    const Job& j = jobs[i];
-    ImgDesc& d = hdesc[i];
-    d.img = j.img;
-    d.mask = j.mask;
-    d.dist = j.dist;
-    d.img_pitch = j.img_pitch;
-    d.mask_pitch = j.mask_pitch;
-    d.dist_pitch = j.dist_pitch;
-    d.width = j.width;
-    d.height = j.height;
-    d.channels = j.channels;
-    d.tiles_x = j.tiles_x();
-    d.tiles_y = j.tiles_y();
-    d.tile_base = base;
-    d.g2 = j.g2;
-    d.v = j.v;
-    d.l_eucl = j.l_eucl;
-    d.l_grad = j.l_grad;
-    d.mode = j.mode;
-    d.ref_fma = j.ref_fma;
+    const dtb_status s = fill_desc(ctx, jobs[i], base, i, &hdesc[i], &htm[2 * i]);
+    if (s != DTB_OK) return s;
     hbase[i] = base;
-    base += (uint32_t)(d.tiles_x * d.tiles_y);
-    if (j.width > 0 && j.height > 0) {
-      const uint32_t bw = j.channels == 3 ? IMG_BOX_RGB : IMG_BOX_GRAY;
-      if (!encode_u8_2d(ctx, &htm[2 * i], j.img, (uint64_t)j.width * j.channels, (uint64_t)j.height, (uint64_t)j.img_pitch,
-                        bw, IMG_BOX_ROWS))
-        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the image layout", i);
-      if (!encode_u8_2d(ctx, &htm[2 * i + 1], j.mask, (uint64_t)j.width, (uint64_t)j.height, (uint64_t)j.mask_pitch, TILE,
-                        TILE))
-        return fail(ctx, DTB_ERR_INVALID_ARG, "image %d: cuTensorMapEncodeTiled rejected the mask layout", i);
-    }
+    base += (uint32_t)(hdesc[i].tiles_x * hdesc[i].tiles_y);
   }
   hbase[n] = base;
   return DTB_OK;

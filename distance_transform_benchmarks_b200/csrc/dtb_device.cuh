@@ -349,10 +349,10 @@ __device__ __forceinline__ uint32_t queue_pop(const Queue& q) {
         b = (base + f) & q.nb_mask;
       }
       const uint32_t h = atomicAdd(&q.hdr->heads[b].v, 1u);
-      __threadfence();  // the ticket before the checks below (pairs with the fence of signal_done_warp)
-      if (ld_volatile(&q.hdr->done.v) | ld_volatile(&q.hdr->error.v)) res = POP_NONE;
-      else if (ld_volatile(&q.hdr->pending.v) == 0u) res = POP_NONE;  // nothing queued at all
-      else res = slot_take(q, b, h, w);
+      // No fence and no checks between the ticket and the slot: with work queued the item is usually in the
+      // slot already, and the end of the queue (done, an error, nothing pending) is noticed by slot_take's
+      // periodic checks within POLL_CHECK_NS even when the ticket came after signal_done_warp read the heads.
+      res = slot_take(q, b, h, w);
     }
     res = __shfl_sync(~0u, res, 0);
     if (res != POP_RESCAN) return res;

@@ -188,6 +188,9 @@ ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, u
 dtb_status reset_queue(dtb_context ctx, uint8_t* dbase, const ScratchLayout& L, cudaStream_t stream);
 // Host image of [descriptors | tensor maps | tile prefix] (bytes o_desc .. o_act of the layout).
 dtb_status build_tables(dtb_context ctx, const std::vector<Job>& jobs, const ScratchLayout& L, std::vector<uint8_t>& out);
+// Descriptor and tensor maps (image box, mask tile) of one image whose tile ids start at tile_base; `index`
+// names the image in error messages.
+dtb_status fill_desc(dtb_context ctx, const Job& j, uint32_t tile_base, int index, ImgDesc* d, CUtensorMap* tm);
 // Total tiles of the jobs (error if beyond the 31-bit tile id space).
 dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* total);
 // Resident warps of the tile kernel of `mode` under `t`.

@@ -8,6 +8,10 @@
 // into the resident mask and warm-starts from the previous map -- every tile starts as already computed and
 // only the tiles the new disks touch are queued.  This is exact: added seeds only lower distances, and the
 // relaxation from the previous fixpoint ends in the fixpoint of the union of the seeds.
+//
+// With dtb_serve_config.live the worker runs no waves: it publishes each request into the device ring of the
+// live tile kernel (dtb_live.cuh), keeps that kernel launched while requests are in flight, watches the
+// completion words the kernel writes into mapped host memory and copies each finished map out.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,12 +21,13 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <vector>
 
 #include "dtb.h"
 #include "dtb_internal.h"
-#include "dtb_kernels.cuh"
+#include "dtb_live.cuh"
 
 namespace dtb {
 
@@ -153,7 +158,9 @@ struct Resident {
   int64_t img_pitch = 0, mask_pitch = 0, dist_pitch = 0;
   size_t o_img = 0, o_mask = 0, o_dist = 0;  // within the block
   uint64_t last_use = 0;
-  int64_t wave = -1;  // wave the image takes part in (busy while it runs)
+  int64_t wave = -1;  // wave the image takes part in (busy while it runs); live engine: 0 while in flight
+  int32_t slot = -1;  // live engine: image slot (descriptor, tensor maps, request counters)
+  uint32_t tile_base = 0, tiles = 0;  // live engine: the image's range of the tile space
 };
 
 struct Request {
@@ -197,6 +204,9 @@ constexpr uint32_t SERVE_MAX_WAVE_TILES = 1u << 20;
 constexpr uint64_t SERVE_WAVE_STAGE_BYTES = 256ull << 20;
 constexpr size_t SERVE_MAX_WAVE_DISKS = 65536;
 
+struct LiveEngine;
+void live_free_resident(LiveEngine* L, const Resident& r);
+
 struct dtb_server_s {
   dtb_context ctx = nullptr;
   dtb_serve_config cfg{};
@@ -222,6 +232,7 @@ struct dtb_server_s {
   size_t stage_cap = SERVE_WAVE_STAGE_BYTES;
   uint32_t workers = 0;  // resident warps of the largest tile-kernel launch
   uint32_t nb = 1;       // priority buckets of the waves' tile queues
+  LiveEngine* live = nullptr;  // live admission instead of waves
 };
 
 namespace {
@@ -242,23 +253,33 @@ bool referenced(dtb_server s, int64_t id) {
   return false;
 }
 
+// Forgets a resident image: its arena block and, in the live engine, its slot and tile range.  Caller holds mu.
+void drop_resident(dtb_server s, std::map<int64_t, Resident>::iterator it) {
+  s->arena.release(it->second.off, it->second.bytes);
+  if (s->live) live_free_resident(s->live, it->second);
+  s->resident.erase(it);
+}
+
+// Least-recently-used idle resident, or resident.end().  Caller holds mu.
+std::map<int64_t, Resident>::iterator lru_idle(dtb_server s) {
+  auto victim = s->resident.end();
+  uint64_t oldest = UINT64_MAX;
+  for (auto it = s->resident.begin(); it != s->resident.end(); ++it) {
+    if (it->second.wave >= s->busy_from || referenced(s, it->first)) continue;
+    if (it->second.last_use < oldest) {
+      oldest = it->second.last_use;
+      victim = it;
+    }
+  }
+  return victim;
+}
+
 // Makes room for `bytes` in the arena by evicting least-recently-used idle residents.  Caller holds mu.
 bool make_room(dtb_server s, size_t bytes, size_t* off) {
   while (!s->arena.alloc(bytes, off)) {
-    int64_t victim = 0;
-    uint64_t oldest = UINT64_MAX;
-    bool found = false;
-    for (auto& kv : s->resident) {
-      if (kv.second.wave >= s->busy_from || referenced(s, kv.first)) continue;
-      if (kv.second.last_use < oldest) {
-        oldest = kv.second.last_use;
-        victim = kv.first;
-        found = true;
-      }
-    }
-    if (!found) return false;
-    s->arena.release(s->resident[victim].off, s->resident[victim].bytes);
-    s->resident.erase(victim);
+    auto victim = lru_idle(s);
+    if (victim == s->resident.end()) return false;
+    drop_resident(s, victim);
     s->st.evictions += 1;
   }
   return true;
@@ -273,6 +294,7 @@ std::vector<Request> admit(dtb_server s, bool* split) {
   const auto now = Clock::now();
   bool blocked = false;  // a new image that did not fit keeps later new images waiting (arrival order)
   bool closed = false;   // a per-wave limit was reached: the rest waits for the next wave
+  std::set<int64_t> kept_new;  // new images left pending: edits of them wait too
   uint64_t w_tiles = 0;
   size_t w_stage = 0, w_disks = 0;
   *split = false;
@@ -286,6 +308,10 @@ std::vector<Request> admit(dtb_server s, bool* split) {
     }
     auto it = s->resident.find(q.r.image_id);
     if (q.r.kind == DTB_REQ_EDIT) {
+      if (it == s->resident.end() && kept_new.count(q.r.image_id)) {
+        keep.push_back(std::move(q));  // its image's request waits: so does the edit
+        continue;
+      }
       if (it == s->resident.end()) {
         complete(s, q, DTB_ERR_INVALID_ARG, now);  // not resident (never submitted, released or evicted)
         continue;
@@ -314,6 +340,7 @@ std::vector<Request> admit(dtb_server s, bool* split) {
       continue;
     }
     if (blocked) {
+      kept_new.insert(q.r.image_id);
       keep.push_back(std::move(q));
       continue;
     }
@@ -347,6 +374,7 @@ std::vector<Request> admit(dtb_server s, bool* split) {
     size_t off = 0;
     if (!make_room(s, r.bytes, &off)) {
       blocked = true;
+      kept_new.insert(q.r.image_id);
       keep.push_back(std::move(q));
       continue;
     }
@@ -583,10 +611,7 @@ void retire_wave(dtb_server s, InFlight& f, dtb_status status) {
   for (const Request& q : f.reqs) {
     if (status != DTB_OK && q.r.kind == DTB_REQ_IMAGE) {
       auto it = s->resident.find(q.r.image_id);
-      if (it != s->resident.end()) {
-        s->arena.release(it->second.off, it->second.bytes);
-        s->resident.erase(it);
-      }
+      if (it != s->resident.end()) drop_resident(s, it);
     }
     complete(s, q, status, now);
   }
@@ -690,6 +715,626 @@ void worker_main(dtb_server s) {
   }
 }
 
+}  // namespace
+
+// ======================================================================================================
+// Live engine (dtb_serve_config.live): requests join the tile queue of one running kernel (dtb_live.cuh).
+// ======================================================================================================
+
+// Pinned staging of one entry: its descriptor and tensor maps, the entry and the published count, copied in
+// on s_in in that order.  Entry e's staging is reused by entry e + LIVE_RING, published only after e ended.
+constexpr size_t LIVE_STAGE = 512;
+constexpr size_t LST_DESC = 0, LST_TMAP = 128, LST_ENTRY = 384, LST_PUB = 448;
+static_assert(LST_TMAP + 2 * sizeof(CUtensorMap) <= LST_ENTRY && LST_ENTRY + sizeof(LiveEntry) <= LST_PUB &&
+                  sizeof(ImgDesc) <= LST_TMAP, "live staging layout");
+constexpr uint32_t LIVE_WATCH_MS = 2000;       // no-progress limit of the live kernel's watchdog
+constexpr uint32_t LIVE_LIFE_US = 4000000;     // a launch claims new requests for this long, then drains and ends
+constexpr uint32_t LIVE_IDLE_US = 20000;       // default idle time after which a launch ends
+constexpr uint32_t LIVE_DISK_CAP = 1u << 20;   // disks of edits in flight
+constexpr int LIVE_CTAS = 3;                   // CTAs of PERSIST_WPC warps per SM (the 168-register launch)
+
+// A published request.
+struct LiveFlight {
+  Request q;
+  uint32_t entry = 0;
+  int stage = 0;               // 0: published; 1: its map is being copied out
+  Clock::time_point t_pub, t_seen;
+  cudaEvent_t ev = nullptr;    // end of the copy out
+  size_t disk_off = SIZE_MAX;  // bytes of the disk pool held by an edit
+  size_t disk_bytes = 0;
+};
+
+struct LiveEngine {
+  uint8_t* dmem = nullptr;     // one device block: queue header, live header, ring, states, tables, entries, disks
+  QueueHdr* qhdr = nullptr;
+  LiveHdr* lh = nullptr;
+  uint32_t* ring = nullptr;
+  uint32_t ring_cap = 0;
+  uint32_t* states = nullptr;
+  ImgDesc* descs = nullptr;
+  CUtensorMap* tmaps = nullptr;
+  LiveSlot* slots = nullptr;
+  LiveEntry* entries = nullptr;
+  int32_t* disks = nullptr;
+  uint32_t tile_cap = 0, nslots = 0;
+  uint32_t* hdone = nullptr;   // mapped pinned host memory (LIVE_RING words), written by the kernel
+  uint32_t* ddone = nullptr;   // its device address
+  uint8_t* hstage = nullptr;   // pinned: LIVE_RING entry stagings, then the disk pool mirror, then constant words
+  int32_t* hdisks = nullptr;
+  uint32_t* hwords = nullptr;  // [0] = 1, [1] = LIVE_WATCH_MS, [2] = injected limit (ms)
+  Arena tiles, diskpool;       // tile-space ranges (4 bytes a tile), disk-pool bytes
+  std::vector<int32_t> free_slots;
+  uint32_t next_entry = 0;
+  std::deque<LiveFlight> flights;  // in publish order
+  uint64_t flight_tiles = 0;
+  std::vector<cudaEvent_t> ev_free;
+  bool running = false;
+  cudaEvent_t ev_kernel = nullptr;
+  uint32_t idle_us = LIVE_IDLE_US;
+  uint32_t grid = 0;
+  uint32_t claimed_seen = 0;   // `claimed` as read after the last launch ended
+};
+
+void live_free_resident(LiveEngine* L, const Resident& r) {
+  if (r.slot >= 0) L->free_slots.push_back(r.slot);
+  if (r.tiles) L->tiles.release(4ull * r.tile_base, 4ull * r.tiles);
+}
+
+namespace {
+
+// Device and pinned allocations of the live engine (dtb_serve_create).
+dtb_status live_create(dtb_server s, uint32_t idle_us) {
+  dtb_context ctx = s->ctx;
+  LiveEngine* L = new (std::nothrow) LiveEngine();
+  if (!L) return DTB_ERR_OUT_OF_MEMORY;
+  s->live = L;
+  s->busy_from = 0;  // a resident is busy while wave == 0
+  L->idle_us = idle_us ? idle_us : LIVE_IDLE_US;
+  // Tile space: every gray pixel the budget can hold, plus 64 tiles of rounding per slot; slots: at most
+  // LIVE_MAX_SLOTS, at least enough for 64 KiB per image.
+  const uint64_t budget = s->cfg.hbm_budget_bytes;
+  L->nslots = (uint32_t)std::min<uint64_t>(LIVE_MAX_SLOTS, std::max<uint64_t>(64, budget / 65536));
+  const uint64_t tiles = budget / (9ull * 1024ull) + 64ull * L->nslots + 64;
+  L->tile_cap = (uint32_t)std::min<uint64_t>(LIVE_MAX_TILES, align_up(tiles, 64));
+  // The live kernel's launch: LIVE_CTAS CTAs per SM, or fewer if fewer fit (the launch is cooperative).
+  const void* fn = (const void*)ggdt_live<PERSIST_WPC, LIVE_CTAS>;
+  int per_sm = 0;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PERSIST_SMEM) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PERSIST_WPC * 32, PERSIST_SMEM) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return fail(ctx, DTB_ERR_CUDA, "serve (live): the live tile kernel cannot be resident");
+  }
+  L->grid = (uint32_t)ctx->num_sms * (uint32_t)std::min(per_sm, LIVE_CTAS);
+  const uint32_t workers = L->grid * PERSIST_WPC;
+  // Ring: items in flight (tiles of the requests in flight, their set-up jobs) plus waiting workers.
+  const uint64_t items = (uint64_t)s->max_tiles + 2ull * (s->max_tiles / LIVE_JOB_TILES + (uint64_t)s->max_reqs) +
+                         workers + 64;
+  uint32_t cap = 1;
+  while (cap < 2 * items && cap < (1u << 30)) cap <<= 1;
+  L->ring_cap = cap;
+  size_t off = 0;
+  const size_t o_q = off;       off = align_up(off + sizeof(QueueHdr), 256);
+  const size_t o_lh = off;      off = align_up(off + sizeof(LiveHdr), 256);
+  const size_t o_ring = off;    off = align_up(off + 4ull * cap, 256);
+  const size_t o_states = off;  off = align_up(off + 4ull * L->tile_cap, 256);
+  const size_t o_desc = off;    off = align_up(off + sizeof(ImgDesc) * L->nslots, 256);
+  const size_t o_tmap = off;    off = align_up(off + 2 * sizeof(CUtensorMap) * L->nslots, 256);
+  const size_t o_slots = off;   off = align_up(off + sizeof(LiveSlot) * L->nslots, 256);
+  const size_t o_ent = off;     off = align_up(off + sizeof(LiveEntry) * LIVE_RING, 256);
+  const size_t o_disks = off;   off = align_up(off + 12ull * LIVE_DISK_CAP, 256);
+  if (cudaMalloc((void**)&L->dmem, off) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "serve (live): cudaMalloc of %zu bytes failed", off);
+  }
+  L->qhdr = reinterpret_cast<QueueHdr*>(L->dmem + o_q);
+  L->lh = reinterpret_cast<LiveHdr*>(L->dmem + o_lh);
+  L->ring = reinterpret_cast<uint32_t*>(L->dmem + o_ring);
+  L->states = reinterpret_cast<uint32_t*>(L->dmem + o_states);
+  L->descs = reinterpret_cast<ImgDesc*>(L->dmem + o_desc);
+  L->tmaps = reinterpret_cast<CUtensorMap*>(L->dmem + o_tmap);
+  L->slots = reinterpret_cast<LiveSlot*>(L->dmem + o_slots);
+  L->entries = reinterpret_cast<LiveEntry*>(L->dmem + o_ent);
+  L->disks = reinterpret_cast<int32_t*>(L->dmem + o_disks);
+  const size_t hbytes = LIVE_STAGE * LIVE_RING + 12ull * LIVE_DISK_CAP + 256;
+  if (cudaHostAlloc((void**)&L->hstage, hbytes, cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void**)&L->hdone, 4ull * LIVE_RING, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer((void**)&L->ddone, L->hdone, 0) != cudaSuccess ||
+      cudaEventCreateWithFlags(&L->ev_kernel, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "serve (live): pinned host buffers");
+  }
+  std::memset(L->hstage, 0, hbytes);
+  std::memset(L->hdone, 0, 4ull * LIVE_RING);
+  L->hdisks = reinterpret_cast<int32_t*>(L->hstage + LIVE_STAGE * LIVE_RING);
+  L->hwords = reinterpret_cast<uint32_t*>(L->hstage + LIVE_STAGE * LIVE_RING + 12ull * LIVE_DISK_CAP);
+  L->hwords[0] = 1u;
+  L->hwords[1] = LIVE_WATCH_MS;
+  L->tiles.reset(4ull * L->tile_cap);
+  L->diskpool.reset(12ull * LIVE_DISK_CAP);
+  for (int32_t k = (int32_t)L->nslots - 1; k >= 0; --k) L->free_slots.push_back(k);
+  // Everything starts at zero (states, counters, entries); the watchdog limit is set once.
+  DTB_CUDA(ctx, cudaMemsetAsync(L->dmem, 0, off, s->s_run));
+  DTB_CUDA(ctx, cudaMemcpyAsync(&L->lh->watch_ms.v, &L->hwords[1], 4, cudaMemcpyHostToDevice, s->s_run));
+  DTB_CUDA(ctx, cudaStreamSynchronize(s->s_run));
+  return DTB_OK;
+}
+
+void live_destroy(LiveEngine* L) {
+  if (!L) return;
+  for (cudaEvent_t e : L->ev_free) cudaEventDestroy(e);
+  for (LiveFlight& f : L->flights)
+    if (f.ev) cudaEventDestroy(f.ev);
+  if (L->ev_kernel) cudaEventDestroy(L->ev_kernel);
+  if (L->dmem) cudaFree(L->dmem);
+  if (L->hstage) cudaFreeHost(L->hstage);
+  if (L->hdone) cudaFreeHost(L->hdone);
+  delete L;
+}
+
+// A free slot and a tile range for a new image of `tiles` tiles, evicting least-recently-used idle images when
+// needed.  Caller holds mu.
+bool live_place(dtb_server s, uint32_t tiles, int32_t* slot, uint32_t* tile_base) {
+  LiveEngine* L = s->live;
+  size_t toff = 0;
+  for (;;) {
+    const bool have_slot = !L->free_slots.empty();
+    const bool have_tiles = tiles == 0 || L->tiles.alloc(4ull * tiles, &toff);
+    if (have_slot && have_tiles) break;
+    if (have_tiles && tiles) L->tiles.release(toff, 4ull * tiles);
+    auto victim = lru_idle(s);
+    if (victim == s->resident.end()) return false;
+    drop_resident(s, victim);
+    s->st.evictions += 1;
+  }
+  *slot = L->free_slots.back();
+  L->free_slots.pop_back();
+  *tile_base = tiles ? (uint32_t)(toff / 4) : 0u;
+  return true;
+}
+
+// Admission of the live engine (caller holds mu): pending requests in arrival order while the requests and tiles
+// in flight stay within the limits, the disk pool has room and (new images) the arena, a slot and a tile range
+// can be found.  An edit of an image in flight waits; a new image that does not fit keeps later new images
+// waiting.
+std::vector<LiveFlight> live_admit_host(dtb_server s) {
+  LiveEngine* L = s->live;
+  std::vector<LiveFlight> out;
+  std::deque<Request> keep;
+  const auto now = Clock::now();
+  bool blocked = false;
+  std::set<int64_t> kept_new;  // new images left pending: edits of them wait too
+  const size_t max_flights = std::min<size_t>((size_t)s->max_reqs, LIVE_RING / 2);
+  while (!s->pending.empty()) {
+    Request q = std::move(s->pending.front());
+    s->pending.pop_front();
+    if (L->flights.size() + out.size() >= max_flights) {
+      keep.push_back(std::move(q));
+      continue;
+    }
+    auto it = s->resident.find(q.r.image_id);
+    if (q.r.kind == DTB_REQ_EDIT) {
+      if (it == s->resident.end() && kept_new.count(q.r.image_id)) {
+        keep.push_back(std::move(q));  // its image's request waits: so does the edit
+        continue;
+      }
+      if (it == s->resident.end()) {
+        complete(s, q, DTB_ERR_INVALID_ARG, now);
+        continue;
+      }
+      if (it->second.wave >= s->busy_from) {
+        keep.push_back(std::move(q));
+        continue;
+      }
+      LiveFlight f;
+      f.disk_bytes = 12 * (q.disks.size() / 3);
+      if (f.disk_bytes) {
+        size_t doff = 0;
+        if (!L->diskpool.alloc(f.disk_bytes, &doff)) {
+          keep.push_back(std::move(q));
+          continue;
+        }
+        f.disk_off = doff;
+      }
+      it->second.wave = 0;
+      it->second.last_use = ++s->tick;
+      L->flight_tiles += it->second.tiles;
+      f.q = std::move(q);
+      out.push_back(std::move(f));
+      continue;
+    }
+    if (it != s->resident.end()) {
+      complete(s, q, DTB_ERR_INVALID_ARG, now);
+      continue;
+    }
+    if (blocked) {
+      kept_new.insert(q.r.image_id);
+      keep.push_back(std::move(q));
+      continue;
+    }
+    const uint64_t t = tiles_of(q.r.img.width, q.r.img.height);
+    if (t > s->max_tiles || t > (uint64_t)LIVE_JOB_TILES << LIVE_CHUNK_BITS) {
+      complete(s, q, DTB_ERR_CAPACITY, now);
+      continue;
+    }
+    if (L->flight_tiles + t > s->max_tiles) {
+      blocked = true;
+      kept_new.insert(q.r.image_id);
+      keep.push_back(std::move(q));
+      continue;
+    }
+    Resident r;
+    r.W = q.r.img.width;
+    r.H = q.r.img.height;
+    r.C = q.r.img.elem_size;
+    r.g2 = gamma_to_g2(q.r.gamma);
+    r.img_pitch = (int64_t)plane_pitch((size_t)r.W * r.C);
+    r.mask_pitch = (int64_t)plane_pitch((size_t)r.W);
+    r.dist_pitch = (int64_t)align_up(4 * (size_t)std::max(r.W, 1), 128);
+    r.o_img = 0;
+    r.o_mask = align_up((size_t)r.img_pitch * r.H, 256);
+    r.o_dist = r.o_mask + align_up((size_t)r.mask_pitch * r.H, 256);
+    r.bytes = r.o_dist + align_up((size_t)r.dist_pitch * r.H, 256);
+    if (r.bytes > s->cfg.hbm_budget_bytes || t > L->tile_cap) {
+      complete(s, q, DTB_ERR_CAPACITY, now);
+      continue;
+    }
+    size_t off = 0;
+    if (!make_room(s, r.bytes, &off)) {
+      blocked = true;
+      kept_new.insert(q.r.image_id);
+      keep.push_back(std::move(q));
+      continue;
+    }
+    r.off = off;
+    if (!live_place(s, (uint32_t)t, &r.slot, &r.tile_base)) {
+      s->arena.release(off, r.bytes);
+      blocked = true;
+      kept_new.insert(q.r.image_id);
+      keep.push_back(std::move(q));
+      continue;
+    }
+    r.tiles = (uint32_t)t;
+    r.wave = 0;
+    r.last_use = ++s->tick;
+    s->resident[q.r.image_id] = r;
+    L->flight_tiles += t;
+    LiveFlight f;
+    f.q = std::move(q);
+    out.push_back(std::move(f));
+  }
+  s->pending = std::move(keep);
+  return out;
+}
+
+// Copies one admitted request in and publishes it (s_in, in order: data, descriptor + maps, entry, count).  The
+// caller holds the context's lock.
+dtb_status live_publish(dtb_server s, LiveFlight& f, const Resident& r) {
+  dtb_context ctx = s->ctx;
+  LiveEngine* L = s->live;
+  cudaStream_t st = s->s_in;
+  const uint32_t e = L->next_entry;
+  uint8_t* stg = L->hstage + LIVE_STAGE * (e & (LIVE_RING - 1u));
+  LiveEntry* ent = reinterpret_cast<LiveEntry*>(stg + LST_ENTRY);
+  std::memset(ent, 0, sizeof(LiveEntry));
+  ent->slot = (uint32_t)r.slot;
+  uint8_t* base = s->arena_base + r.off;
+  const dtb_serve_request& q = f.q.r;
+  if (q.kind == DTB_REQ_IMAGE) {
+    ent->kind = LIVE_NEW;
+    const size_t rb = (size_t)r.W * r.C;
+    if (r.W > 0 && r.H > 0) {
+      if ((size_t)q.img.pitch == rb && (size_t)r.img_pitch == rb)
+        DTB_CUDA(ctx, cudaMemcpyAsync(base + r.o_img, q.img.buffer, rb * r.H, cudaMemcpyHostToDevice, st));
+      else
+        DTB_CUDA(ctx, cudaMemcpy2DAsync(base + r.o_img, r.img_pitch, q.img.buffer, q.img.pitch, rb, r.H,
+                                        cudaMemcpyHostToDevice, st));
+      if (q.mask.pitch == r.W && r.mask_pitch == r.W)
+        DTB_CUDA(ctx, cudaMemcpyAsync(base + r.o_mask, q.mask.buffer, (size_t)r.W * r.H, cudaMemcpyHostToDevice, st));
+      else
+        DTB_CUDA(ctx, cudaMemcpy2DAsync(base + r.o_mask, r.mask_pitch, q.mask.buffer, q.mask.pitch, r.W, r.H,
+                                        cudaMemcpyHostToDevice, st));
+    }
+    Job j;
+    j.img = base + r.o_img;
+    j.img_pitch = r.img_pitch;
+    j.channels = r.C;
+    j.mask = base + r.o_mask;
+    j.mask_pitch = r.mask_pitch;
+    j.dist = reinterpret_cast<float*>(base + r.o_dist);
+    j.dist_pitch = r.dist_pitch;
+    j.width = r.W;
+    j.height = r.H;
+    j.g2 = r.g2;
+    j.v = s->cfg.v;
+    j.mode = MODE_NS;
+    ImgDesc* d = reinterpret_cast<ImgDesc*>(stg + LST_DESC);
+    CUtensorMap* tm = reinterpret_cast<CUtensorMap*>(stg + LST_TMAP);
+    std::memset(stg, 0, LST_ENTRY);
+    dtb_status ds = fill_desc(ctx, j, r.tile_base, 0, d, tm);
+    if (ds != DTB_OK) return ds;
+    DTB_CUDA(ctx, cudaMemcpyAsync(L->descs + r.slot, d, sizeof(ImgDesc), cudaMemcpyHostToDevice, st));
+    DTB_CUDA(ctx, cudaMemcpyAsync(L->tmaps + 2 * r.slot, tm, 2 * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
+  } else {
+    ent->kind = LIVE_EDIT;
+    const size_t nd = f.q.disks.size() / 3;
+    ent->n_disks = (uint32_t)nd;
+    if (nd) {
+      ent->disk_idx = (uint32_t)(f.disk_off / 12);
+      std::memcpy(reinterpret_cast<uint8_t*>(L->hdisks) + f.disk_off, f.q.disks.data(), 12 * nd);
+      DTB_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<uint8_t*>(L->disks) + f.disk_off,
+                                    reinterpret_cast<uint8_t*>(L->hdisks) + f.disk_off, 12 * nd, cudaMemcpyHostToDevice, st));
+    }
+  }
+  // dtb_debug_inject_queue_stall on the server's context: the next request the kernel claims counts one item
+  // that never runs, under the injected no-progress limit (the caller holds ctx->mu).
+  if (ctx->inject_stall_ns) {
+    L->hwords[2] = (uint32_t)std::max<uint64_t>(1, ctx->inject_stall_ns / 1000000ull);
+    ctx->inject_stall_ns = 0;
+    DTB_CUDA(ctx, cudaMemcpyAsync(&L->lh->watch_ms.v, &L->hwords[2], 4, cudaMemcpyHostToDevice, st));
+    DTB_CUDA(ctx, cudaMemcpyAsync(&L->lh->inject.v, &L->hwords[0], 4, cudaMemcpyHostToDevice, st));
+  }
+  DTB_CUDA(ctx, cudaMemcpyAsync(L->entries + (e & (LIVE_RING - 1u)), ent, sizeof(LiveEntry), cudaMemcpyHostToDevice, st));
+  uint32_t* pub = reinterpret_cast<uint32_t*>(stg + LST_PUB);
+  *pub = e + 1u;
+  DTB_CUDA(ctx, cudaMemcpyAsync(&L->lh->published.v, pub, 4, cudaMemcpyHostToDevice, st));
+  f.entry = e;
+  L->next_entry = e + 1u;
+  return DTB_OK;
+}
+
+// Launches the live kernel (queue header and ring reset first, on the tile-run stream).
+dtb_status live_launch(dtb_server s) {
+  dtb_context ctx = s->ctx;
+  LiveEngine* L = s->live;
+  cudaStream_t st = s->s_run;
+  DTB_CUDA(ctx, cudaMemsetAsync(L->qhdr, 0, sizeof(QueueHdr), st));
+  DTB_CUDA(ctx, cudaMemsetAsync(L->ring, 0, 4ull * L->ring_cap, st));
+  LiveArgs a{};
+  a.q.hdr = L->qhdr;
+  a.q.ring = L->ring;
+  a.q.mask = L->ring_cap - 1u;
+  a.q.timeout_ns = (uint64_t)LIVE_WATCH_MS * 1000000ull;
+  a.q.max_visits = 0xF0000000u;
+  a.q.total_tiles = L->tile_cap;
+  a.states = L->states;
+  a.descs = L->descs;
+  a.tmaps = L->tmaps;
+  a.lh = L->lh;
+  a.slots = L->slots;
+  a.entries = L->entries;
+  a.disks = L->disks;
+  a.host_done = L->ddone;
+  a.nslots = L->nslots;
+  a.disk_cap = LIVE_DISK_CAP;
+  a.idle_us = L->idle_us;
+  a.life_us = LIVE_LIFE_US;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(L->grid);
+  cfg.blockDim = dim3(PERSIST_WPC * 32);
+  cfg.dynamicSmemBytes = PERSIST_SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;  // co-residency of all workers (the slot waits need it)
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  void* args[1] = {(void*)&a};
+  DTB_CUDA(ctx, cudaLaunchKernelExC(&cfg, (const void*)ggdt_live<PERSIST_WPC, LIVE_CTAS>, args));
+  DTB_CUDA(ctx, cudaEventRecord(L->ev_kernel, st));
+  L->running = true;
+  return DTB_OK;
+}
+
+// A launch has ended: its error (if any) fails the requests it claimed and did not finish (their images are
+// dropped: their tile states are not trustworthy); unclaimed requests stay for the next launch.
+void live_after_kernel(dtb_server s) {
+  dtb_context ctx = s->ctx;
+  LiveEngine* L = s->live;
+  L->running = false;
+  QueueHdr h{};
+  LiveHdr lhh{};
+  dtb_status status = DTB_OK;
+  if (cudaEventSynchronize(L->ev_kernel) != cudaSuccess ||
+      cudaMemcpy(&h, L->qhdr, sizeof(QueueHdr), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&lhh, L->lh, sizeof(LiveHdr), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    status = DTB_ERR_CUDA;
+  } else if (h.error.v) {
+    status = h.error.v == DERR_QUEUE_TIMEOUT || h.error.v == DERR_TMA_TIMEOUT || h.error.v == DERR_RING_FULL
+                 ? DTB_ERR_TIMEOUT
+                 : DTB_ERR_DEVICE;
+    std::lock_guard<std::mutex> ctx_lock(ctx->mu);
+    fail(ctx, status, "serve (live): device error %u (detail %u)", h.error.v, h.err_info.v);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->st.tile_visits += h.progress.v;
+  L->claimed_seen = lhh.claimed.v;
+  if (status == DTB_OK) return;
+  // Requests claimed by the failed launch (entries below `claimed`) whose completion word is not written fail.
+  const auto now = Clock::now();
+  for (auto it = L->flights.begin(); it != L->flights.end();) {
+    LiveFlight& f = *it;
+    const bool claimed = status == DTB_ERR_CUDA || (int32_t)(lhh.claimed.v - f.entry) > 0;
+    const bool finished = L->hdone[f.entry & (LIVE_RING - 1u)] == f.entry + 1u;
+    if (f.stage != 0 || !claimed || finished) {
+      ++it;
+      continue;
+    }
+    auto r = s->resident.find(f.q.r.image_id);
+    if (r != s->resident.end()) {
+      L->flight_tiles -= r->second.tiles;
+      drop_resident(s, r);
+    }
+    if (f.disk_off != SIZE_MAX) L->diskpool.release(f.disk_off, f.disk_bytes);
+    complete(s, f.q, status, now);
+    it = L->flights.erase(it);
+  }
+  // The next launch starts from the default watchdog limit.
+  if (cudaMemcpyAsync(&L->lh->watch_ms.v, &L->hwords[1], 4, cudaMemcpyHostToDevice, s->s_run) != cudaSuccess)
+    cudaGetLastError();
+  s->cv_done.notify_all();
+}
+
+void live_worker_main(dtb_server s) {
+  cudaSetDevice(s->ctx->device);
+  LiveEngine* L = s->live;
+  for (;;) {
+    std::vector<LiveFlight> adm;
+    std::vector<Resident> rs;
+    Clock::time_point t0 = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->stop && s->pending.empty() && L->flights.empty()) break;
+      adm = live_admit_host(s);
+      for (LiveFlight& f : adm) {
+        rs.push_back(s->resident[f.q.r.image_id]);
+        const double w = std::chrono::duration<double, std::milli>(t0 - f.q.t_submit).count();
+        s->st.queue_wait_ms += w;
+        s->st.queue_wait_max_ms = std::max(s->st.queue_wait_max_ms, w);
+      }
+      if (!adm.empty()) s->cv_done.notify_all();  // admission may have completed invalid requests
+    }
+    bool progress = !adm.empty();
+    // Publish the admitted requests.
+    for (size_t i = 0; i < adm.size(); ++i) {
+      dtb_status ps;
+      {
+        std::lock_guard<std::mutex> ctx_lock(s->ctx->mu);
+        ps = live_publish(s, adm[i], rs[i]);
+      }
+      adm[i].t_pub = Clock::now();
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->st.host_prep_ms += std::chrono::duration<double, std::milli>(adm[i].t_pub - t0).count() / (double)adm.size();
+      if (ps != DTB_OK) {
+        // Nothing was published for it (the count is copied last); its copies in may still run: wait for them.
+        cudaStreamSynchronize(s->s_in);
+        auto r = s->resident.find(adm[i].q.r.image_id);
+        if (r != s->resident.end()) {
+          L->flight_tiles -= r->second.tiles;
+          if (adm[i].q.r.kind == DTB_REQ_IMAGE) drop_resident(s, r);
+          else r->second.wave = -1;
+        }
+        if (adm[i].disk_off != SIZE_MAX) L->diskpool.release(adm[i].disk_off, adm[i].disk_bytes);
+        complete(s, adm[i].q, ps, Clock::now());
+        s->cv_done.notify_all();
+        continue;
+      }
+      L->flights.push_back(std::move(adm[i]));
+    }
+    // The kernel: notice its end; launch it while published requests wait.
+    if (L->running && cudaEventQuery(L->ev_kernel) != cudaErrorNotReady) {
+      live_after_kernel(s);
+      progress = true;
+    }
+    if (!L->running) {
+      bool waiting = false;
+      for (const LiveFlight& f : L->flights)
+        if (f.stage == 0 && L->hdone[f.entry & (LIVE_RING - 1u)] != f.entry + 1u) waiting = true;
+      if (waiting) {
+        dtb_status ls;
+        {
+          std::lock_guard<std::mutex> ctx_lock(s->ctx->mu);
+          ls = live_launch(s);
+        }
+        if (ls == DTB_OK) {
+          std::lock_guard<std::mutex> lk(s->mu);
+          s->st.waves += 1;  // launches of the live kernel
+        } else {
+          // Could not launch: fail the requests that wait for it.
+          cudaStreamSynchronize(s->s_in);
+          std::lock_guard<std::mutex> lk(s->mu);
+          for (auto it = L->flights.begin(); it != L->flights.end();) {
+            if (it->stage != 0) { ++it; continue; }
+            auto r = s->resident.find(it->q.r.image_id);
+            if (r != s->resident.end()) {
+              L->flight_tiles -= r->second.tiles;
+              drop_resident(s, r);
+            }
+            if (it->disk_off != SIZE_MAX) L->diskpool.release(it->disk_off, it->disk_bytes);
+            complete(s, it->q, ls, Clock::now());
+            it = L->flights.erase(it);
+          }
+          s->cv_done.notify_all();
+        }
+        progress = true;
+      }
+    }
+    // Finished maps: copy out.
+    for (LiveFlight& f : L->flights) {
+      if (f.stage != 0 || L->hdone[f.entry & (LIVE_RING - 1u)] != f.entry + 1u) continue;
+      f.t_seen = Clock::now();
+      std::lock_guard<std::mutex> lk(s->mu);
+      const Resident& r = s->resident[f.q.r.image_id];
+      const dtb_image& o = f.q.r.out;
+      if (L->ev_free.empty()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) cudaGetLastError();
+        L->ev_free.push_back(e);
+      }
+      f.ev = L->ev_free.back();
+      L->ev_free.pop_back();
+      bool ok = f.ev != nullptr;
+      if (ok && o.width > 0 && o.height > 0)
+        ok = cudaMemcpy2DAsync(o.buffer, o.pitch, s->arena_base + r.off + r.o_dist, r.dist_pitch, 4 * (size_t)o.width,
+                               o.height, cudaMemcpyDeviceToHost, s->s_out) == cudaSuccess;
+      ok = ok && cudaEventRecord(f.ev, s->s_out) == cudaSuccess;
+      if (!ok) {
+        cudaGetLastError();
+        if (f.ev) L->ev_free.push_back(f.ev);
+        f.ev = nullptr;
+      }
+      f.stage = 1;
+      progress = true;
+    }
+    // Copies out that ended: the request completes and its image is free for the next request.
+    for (auto it = L->flights.begin(); it != L->flights.end();) {
+      LiveFlight& f = *it;
+      if (f.stage != 1) { ++it; continue; }
+      dtb_status status = DTB_OK;
+      if (f.ev) {
+        const cudaError_t q = cudaEventQuery(f.ev);
+        if (q == cudaErrorNotReady) { ++it; continue; }
+        if (q != cudaSuccess) { cudaGetLastError(); status = DTB_ERR_CUDA; }
+        L->ev_free.push_back(f.ev);
+      } else {
+        status = DTB_ERR_CUDA;
+      }
+      const auto now = Clock::now();
+      std::lock_guard<std::mutex> lk(s->mu);
+      auto r = s->resident.find(f.q.r.image_id);
+      if (r != s->resident.end()) {
+        L->flight_tiles -= r->second.tiles;
+        s->st.tiles += r->second.tiles;
+        r->second.wave = -1;
+        if (status != DTB_OK && f.q.r.kind == DTB_REQ_IMAGE) drop_resident(s, r);
+      }
+      if (f.disk_off != SIZE_MAX) L->diskpool.release(f.disk_off, f.disk_bytes);
+      s->st.kernel_ms += std::chrono::duration<double, std::milli>(f.t_seen - f.t_pub).count();
+      s->st.copy_out_ms += std::chrono::duration<double, std::milli>(now - f.t_seen).count();
+      complete(s, f.q, status, now);
+      s->cv_done.notify_all();
+      it = L->flights.erase(it);
+      progress = true;
+    }
+    if (!progress) {
+      std::unique_lock<std::mutex> lk(s->mu);
+      const bool idle = L->flights.empty() && !L->running;
+      if (idle) s->cv_sub.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+      else s->cv_sub.wait_for(lk, std::chrono::microseconds(20));
+    }
+  }
+  // Ask a running kernel to end, and wait for it (bounded by its idle time).
+  if (L->running) {
+    if (cudaMemcpyAsync(&L->lh->stop.v, &L->hwords[0], 4, cudaMemcpyHostToDevice, s->s_in) != cudaSuccess) cudaGetLastError();
+    live_after_kernel(s);
+  }
+}
+
+}  // namespace
+
+namespace {
+
 // Frees the server's device and host resources (no wave in flight).
 void release_server(dtb_server s) {
   for (WaveSlot& w : s->slot) {
@@ -699,6 +1344,7 @@ void release_server(dtb_server s) {
     for (cudaEvent_t e : {w.ev_in, w.ev_comp, w.ev_done, w.t_in0, w.t_in1, w.t_run0, w.t_run1, w.t_out0, w.t_out1})
       if (e) cudaEventDestroy(e);
   }
+  live_destroy(s->live);
   for (cudaStream_t t : {s->s_in, s->s_run, s->s_out})
     if (t) cudaStreamDestroy(t);
   if (s->arena_base) cudaFree(s->arena_base);
@@ -711,7 +1357,7 @@ extern "C" {
 
 DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg, dtb_server* out) {
   if (!ctx || !cfg || !out || cfg->hbm_budget_bytes == 0 || !(cfg->v >= 0.0f) || cfg->max_wave_requests < 0 ||
-      cfg->max_wave_tiles > (1u << 26))
+      cfg->max_wave_tiles > (1u << 26) || (cfg->live != 0 && cfg->live != 1))
     return DTB_ERR_INVALID_ARG;
   *out = nullptr;
   dtb_server s = new (std::nothrow) dtb_server_s();
@@ -747,6 +1393,17 @@ DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg
   s->max_reqs = cfg->max_wave_requests > 0 ? cfg->max_wave_requests : SERVE_MAX_WAVE_REQUESTS;
   s->max_tiles = cfg->max_wave_tiles > 0 ? cfg->max_wave_tiles : SERVE_MAX_WAVE_TILES;
   s->stage_cap = cfg->wave_stage_bytes > 0 ? (size_t)cfg->wave_stage_bytes : (size_t)SERVE_WAVE_STAGE_BYTES;
+  if (cfg->live) {
+    // Live admission: the live kernel's tables, ring and pinned buffers instead of per-wave slots.
+    const dtb_status ls = live_create(s, cfg->live_idle_us);
+    if (ls != DTB_OK) {
+      release_server(s);
+      return ls;
+    }
+    s->worker = std::thread(live_worker_main, s);
+    *out = s;
+    return DTB_OK;
+  }
   for (int k = 0; k < NS_VARIANTS; ++k) {
     LaunchTuning t = ctx->tuning;
     t.variant = k;
@@ -832,8 +1489,7 @@ DTB_API dtb_status dtb_serve_release(dtb_server s, int64_t image_id) {
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->resident.find(image_id);
   if (it == s->resident.end() || it->second.wave >= s->busy_from || referenced(s, image_id)) return DTB_ERR_INVALID_ARG;
-  s->arena.release(it->second.off, it->second.bytes);
-  s->resident.erase(it);
+  drop_resident(s, it);
   return DTB_OK;
 }
 

@@ -187,7 +187,15 @@ DTB_API dtb_status dtb_context_set_tuning_cache(dtb_context ctx, const char* pat
  * dtb_serve_create allocates everything the engine uses: the resident arena (hbm_budget_bytes) and, for each of
  * the two waves that can be in flight, its scratch, staging and pinned table buffers, sized by the per-wave
  * limits of the config; a wave that would exceed a limit is closed and the rest waits for the next wave, so no
- * allocation and no device-wide synchronisation happens while waves run.  An edit may add at most 65536 disks. */
+ * allocation and no device-wide synchronisation happens while waves run.  An edit may add at most 65536 disks.
+ * With live = 1 there are no waves: one persistent tile kernel keeps running while requests flow, and each
+ * request is published into a device ring once its image is copied in; idle warps of the running kernel claim
+ * it and queue its work beside the tiles of the requests already running (a new image's set-up -- tile states
+ * and the seed scan -- runs as kernel jobs; an edit draws its disks and queues the tiles they touch), so a
+ * request never waits for another to end.  Each request's completion is signalled by the kernel itself, and
+ * its map is copied out while the kernel goes on.  The kernel occupies every SM while it runs and ends after
+ * live_idle_us without work; the engine launches it again for the next request.  The live tile queue is one
+ * FIFO ring.  A request whose run fails (a device error, or dtb_debug_inject_queue_stall) drops its image. */
 #define DTB_REQ_IMAGE 0  /* new image: img (gray / rgb8), mask, gamma; resident under image_id afterwards */
 #define DTB_REQ_EDIT 1   /* seed edit of the resident image image_id: n_disks disks (cx, cy, r) added */
 typedef struct dtb_serve_config {
@@ -197,6 +205,11 @@ typedef struct dtb_serve_config {
   uint32_t max_wave_tiles;    /* at most this many 32 x 32 tiles per wave (0 = 2^20); an image alone above it is
                                  rejected with DTB_ERR_CAPACITY */
   uint64_t wave_stage_bytes;  /* device staging per wave for new images whose rows need a new pitch (0 = 256 MiB) */
+  int32_t live;               /* 0: waves; 1: live admission -- requests join the tile queue of one persistent kernel
+                                 that keeps running, and max_wave_requests / max_wave_tiles bound the requests and
+                                 tiles in flight at once */
+  uint32_t live_idle_us;      /* live: the kernel ends after this long with nothing queued and nothing claimed
+                                 (0 = 20000); the next request launches it again */
 } dtb_serve_config;
 typedef struct dtb_serve_request {
   int32_t kind;

@@ -2,7 +2,8 @@
 
 A new-image request must equal a cold run of its image and mask; a seed edit must equal a cold run with the
 union of the image's original seeds and every disk added to it so far (warm starts are exact because added
-seeds only lower distances).
+seeds only lower distances).  The tests that apply to both engines run with waves (live=False) and with live
+admission into a running tile kernel (live=True).
 """
 import time
 
@@ -41,10 +42,14 @@ def _mask_with(mask, disks):
     return mask | wl.disks_mask(w, h, [(x, y) for x, y, _ in disks], [r for _, _, r in disks])
 
 
-def test_requests_in_the_mix_match_the_oracle_and_running_alone():
+BOTH = pytest.mark.parametrize("live", [False, True], ids=["waves", "live"])
+
+
+@BOTH
+def test_requests_in_the_mix_match_the_oracle_and_running_alone(live):
     rng = np.random.default_rng(0)
     batch = _images(31, 8)
-    srv = dtb.Server(256 << 20)
+    srv = dtb.Server(256 << 20, live=live)
     expected, outs = {}, {}
     masks_now = {}
     # all new images at once, then edits submitted while the first waves still run
@@ -73,7 +78,7 @@ def test_requests_in_the_mix_match_the_oracle_and_running_alone():
     srv.close()
     # the same new image alone in its own server gives the same bits
     img, mask, g = batch[4]
-    alone = dtb.Server(64 << 20)
+    alone = dtb.Server(64 << 20, live=live)
     out = torch.empty(img.shape[:2], dtype=torch.float32)
     rid = alone.submit_image(1, torch.from_numpy(img), torch.from_numpy(mask), g, out)
     assert _drain(alone, 1)[rid]["status"] == 0
@@ -82,7 +87,8 @@ def test_requests_in_the_mix_match_the_oracle_and_running_alone():
     alone.close()
 
 
-def test_budget_eviction_and_capacity():
+@BOTH
+def test_budget_eviction_and_capacity(live):
     batch = _images(32, 6, smin=200, smax=260)
     def a128(x):
         return -(-x // 128) * 128
@@ -94,7 +100,7 @@ def test_budget_eviction_and_capacity():
         return h * ((rb if rb % 16 == 0 else a128(rb)) + (w if w % 16 == 0 else a128(w)) + a128(4 * w)) + 3 * 256
 
     per_image = max(planes(i) for i, _, _ in batch)
-    srv = dtb.Server(3 * per_image)
+    srv = dtb.Server(3 * per_image, live=live)
     outs = {}
     for i, (img, mask, g) in enumerate(batch):
         out = torch.empty(img.shape[:2], dtype=torch.float32)
@@ -115,12 +121,14 @@ def test_budget_eviction_and_capacity():
     srv.close()
 
 
-def test_overlapping_small_waves_keep_per_image_order():
+@BOTH
+def test_overlapping_small_waves_keep_per_image_order(live):
     """Two waves in flight at a time: with at most two requests per wave, new images and edits of images whose
-    own wave may still be running (they wait for it) are all exact, edits applied in submission order."""
+    own wave may still be running (they wait for it) are all exact, edits applied in submission order.  Live:
+    at most two requests in flight at once, the same order rule."""
     rng = np.random.default_rng(7)
     batch = _images(33, 24, smin=40, smax=260)
-    srv = dtb.Server(512 << 20, max_wave_requests=2)
+    srv = dtb.Server(512 << 20, max_wave_requests=2, live=live)
     masks_now, outs, expected = {}, {}, {}
 
     def edit(j):
@@ -147,18 +155,21 @@ def test_overlapping_small_waves_keep_per_image_order():
         assert_images_eq(outs[rid], expected[rid], "request %d" % rid)
     st = srv.stats()
     assert st["completed"] == len(outs) and st["failed"] == 0
-    assert st["waves"] >= len(outs) // 2
+    if not live:
+        assert st["waves"] >= len(outs) // 2
     srv.close()
 
 
-def test_failed_wave_fails_its_requests_only():
+@BOTH
+def test_failed_wave_fails_its_requests_only(live):
     """A wave whose tile queue stalls (host-side injection: one phantom queued tile, short no-progress limit;
     no device fault) completes its requests with DTB_ERR_TIMEOUT and drops its new image; the engine keeps
-    serving, and requests before and after it are exact."""
+    serving, and requests before and after it are exact.  Live: the stalled request is the next one the running
+    kernel claims; the kernel ends on its watchdog and the next request launches it again."""
     rng = np.random.default_rng(9)
     batch = _images(35, 3, smin=60, smax=200)
     ctx = dtb.Context(0)
-    srv = dtb.Server(128 << 20, ctx=ctx)
+    srv = dtb.Server(128 << 20, ctx=ctx, live=live)
 
     def new_image(i):
         img, mask, g = batch[i]
@@ -228,4 +239,69 @@ def test_waves_split_at_their_limits_allocate_nothing_and_report_phase_times():
     rid = srv.submit_image(901, torch.from_numpy(img), torch.from_numpy(mask), g, out)
     assert _drain(srv, 1)[rid]["status"] == 0
     assert_images_eq(out, orc.ggdt_ns(img, mask, g), "after a rejected request")
+    srv.close()
+
+
+def test_live_request_admitted_while_another_runs_finishes_first():
+    """Live admission: small requests submitted while a long one (the 4096 x 4096 maze, many re-activation
+    rounds) is on the GPU are claimed by the running kernel and complete before it, all in one launch; each map
+    equals its run alone (the small ones against the oracle, the maze against a one-shot call)."""
+    maze, mmask, mg = wl.config1()
+    small = _images(61, 6, smin=64, smax=200)
+    srv = dtb.Server(1 << 30, live=True, live_idle_us=200000)
+    order = []
+    out_m = torch.empty(maze.shape, dtype=torch.float32).pin_memory()
+    hm, hmm = torch.from_numpy(maze).pin_memory(), torch.from_numpy(mmask).pin_memory()
+    small_in = [(torch.from_numpy(i).pin_memory(), torch.from_numpy(m).pin_memory()) for i, m, _ in small]
+    outs = [torch.empty(i.shape[:2], dtype=torch.float32).pin_memory() for i, _, _ in small]
+    rid_m = srv.submit_image(1, hm, hmm, mg, out_m)
+    time.sleep(0.002)  # the maze is claimed and running
+    rids = [srv.submit_image(10 + k, hi, hk, g, outs[k]) for k, ((hi, hk), (_, _, g)) in enumerate(zip(small_in, small))]
+    t0 = time.time()
+    while len(order) < 1 + len(rids):
+        for c in srv.poll(wait_ms=50):
+            assert c["status"] == 0, c
+            order.append(c["request_id"])
+        assert time.time() - t0 < 60
+    assert order.index(rid_m) == len(order) - 1, order  # every small request ended before the maze
+    st = srv.stats()
+    assert st["waves"] == 1, st  # one launch served them all
+    srv.close()
+    for k, (img, mask, g) in enumerate(small):
+        assert_images_eq(outs[k], orc.ggdt_ns(img, mask, g), "small request %d" % k)
+    ref = dtb.geodesic_distance_transform(torch.from_numpy(maze).cuda(), torch.from_numpy(mmask).cuda(), mg)
+    assert_images_eq(out_m, ref.cpu().numpy(), "maze, live vs one-shot")
+
+
+def test_live_kernel_ends_when_idle_relaunches_and_allocates_nothing():
+    """The live kernel ends after its idle time; the next request launches it again.  Serving allocates no
+    device memory (free memory unchanged across requests and launches), and edits stay exact across launches."""
+    rng = np.random.default_rng(3)
+    batch = _images(62, 4, smin=80, smax=300)
+    srv = dtb.Server(256 << 20, live=True, live_idle_us=2000)
+    hosts = [(torch.from_numpy(i).pin_memory(), torch.from_numpy(m).pin_memory()) for i, m, _ in batch]
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    masks_now = {}
+    for k, ((img, mask, g), (hi, hm)) in enumerate(zip(batch, hosts)):
+        out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+        rid = srv.submit_image(k, hi, hm, g, out)
+        assert _drain(srv, 1)[rid]["status"] == 0
+        assert_images_eq(out, orc.ggdt_ns(img, mask, g), "image %d" % k)
+        masks_now[k] = mask.copy()
+        time.sleep(0.05)  # well past the idle time: the kernel has ended
+    for k in (0, 2, 0):
+        img, _, g = batch[k]
+        disks = _disks(rng, img, 2)
+        masks_now[k] = _mask_with(masks_now[k], disks)
+        out = torch.empty(img.shape[:2], dtype=torch.float32).pin_memory()
+        rid = srv.submit_edit(k, disks, out)
+        assert _drain(srv, 1)[rid]["status"] == 0
+        assert_images_eq(out, orc.ggdt_ns(img, masks_now[k], g), "edit of image %d" % k)
+        time.sleep(0.05)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["waves"] >= 7, st  # a launch per request after each idle end
+    assert st["tile_visits"] > 0 and st["kernel_ms"] > 0
     srv.close()
