@@ -458,6 +458,8 @@ def run_serve(args, dev, pool, live=False):
         r = max(1, b["completed"] - a["completed"])
         if live:
             return {"launches": int(b["waves"] - a["waves"]),
+                    "launch_ends": {k: int(b["live_ended_" + k] - a["live_ended_" + k])
+                                    for k in ("idle", "lifetime", "error", "stop")},
                     "host_prep_ms_per_request": (b["host_prep_ms"] - a["host_prep_ms"]) / r,
                     "in_and_kernel_ms_per_request": (b["kernel_ms"] - a["kernel_ms"]) / r,
                     "copy_out_ms_per_request": (b["copy_out_ms"] - a["copy_out_ms"]) / r,

@@ -54,9 +54,10 @@ class Context:
         self.check(lib().dtb_last_stats(self._h, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in DtbStats._fields_}
 
-    def set_tuning(self, ctas_per_sm=0, grid_percent=0, host_chunk_kpx=0, queue_buckets=0, bucket_width_pct=0, staging=0):
+    def set_tuning(self, ctas_per_sm=0, grid_percent=0, host_chunk_kpx=0, queue_buckets=0, bucket_width_pct=0, staging=0,
+                   warps_per_cta=0):
         """dtb_context_set_tuning: 0 keeps a field (see include/dtb.h for the ranges)."""
-        t = DtbTuning(ctas_per_sm, grid_percent, host_chunk_kpx, queue_buckets, bucket_width_pct, staging)
+        t = DtbTuning(ctas_per_sm, grid_percent, host_chunk_kpx, queue_buckets, bucket_width_pct, staging, warps_per_cta)
         self.check(lib().dtb_context_set_tuning(self._h, ctypes.byref(t)))
 
     def get_tuning(self):

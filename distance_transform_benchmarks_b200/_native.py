@@ -66,7 +66,8 @@ class DtbStats(ctypes.Structure):
 
 class DtbTuning(ctypes.Structure):
     _fields_ = [("ctas_per_sm", ctypes.c_int32), ("grid_percent", ctypes.c_int32), ("host_chunk_kpx", ctypes.c_int32),
-                ("queue_buckets", ctypes.c_int32), ("bucket_width_pct", ctypes.c_int32), ("staging", ctypes.c_int32)]
+                ("queue_buckets", ctypes.c_int32), ("bucket_width_pct", ctypes.c_int32), ("staging", ctypes.c_int32),
+                ("warps_per_cta", ctypes.c_int32)]
 
 
 class DtbServeConfig(ctypes.Structure):
@@ -91,7 +92,9 @@ class DtbServeStats(ctypes.Structure):
                [(n, ctypes.c_uint64) for n in ("resident_bytes", "tiles", "tile_visits")] + \
                [(n, ctypes.c_double) for n in ("host_prep_ms", "copy_in_ms", "kernel_ms", "copy_out_ms", "queue_wait_ms",
                                                "queue_wait_max_ms")] + \
-               [("waves_split", ctypes.c_int64)]
+               [("waves_split", ctypes.c_int64)] + \
+               [(n, ctypes.c_int64) for n in ("live_ended_idle", "live_ended_lifetime", "live_ended_error",
+                                             "live_ended_stop")]
 
 
 class DtbError(RuntimeError):

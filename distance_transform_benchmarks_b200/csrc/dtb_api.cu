@@ -309,7 +309,7 @@ dtb_status count_tiles(dtb_context ctx, const std::vector<Job>& jobs, uint32_t* 
 uint32_t resident_workers(dtb_context ctx, int mode, const LaunchTuning& t) {
   const int bps = mode == MODE_NS ? ctx->ns_blocks_per_sm[t.variant] : ctx->ref_blocks_per_sm;
   const uint32_t ctas = std::max<uint32_t>(1u, (uint32_t)(ctx->num_sms * bps) * (uint32_t)t.grid_percent / 100u);
-  return ctas * PERSIST_WPC;
+  return ctas * (uint32_t)(mode == MODE_NS ? NS_VARIANT_TABLE[t.variant].wpc : PERSIST_WPC);
 }
 
 ScratchLayout layout_for(int n, uint32_t total, uint32_t workers, bool rounds, uint32_t buckets) {
@@ -470,8 +470,9 @@ dtb_status enqueue_persistent(dtb_context ctx, uint8_t* dbase, const ScratchLayo
 dtb_status launch_tile_kernel(dtb_context ctx, int mode, const LaunchTuning& t, const ImgDesc* descs,
                               const CUtensorMap* tmaps, uint32_t* states, const Queue& q, cudaStream_t stream) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(resident_workers(ctx, mode, t) / PERSIST_WPC);
-  cfg.blockDim = dim3(PERSIST_WPC * 32);
+  const int wpc = mode == MODE_NS ? NS_VARIANT_TABLE[t.variant].wpc : PERSIST_WPC;
+  cfg.gridDim = dim3(resident_workers(ctx, mode, t) / (uint32_t)wpc);
+  cfg.blockDim = dim3((uint32_t)wpc * 32u);
   cfg.dynamicSmemBytes = mode == MODE_NS ? ctx->ns_smem[t.variant] : PERSIST_SMEM;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
@@ -695,6 +696,7 @@ void tuning_to_abi(dtb_context ctx, const LaunchTuning& lt, dtb_tuning* t) {
   t->queue_buckets = lt.buckets;
   t->bucket_width_pct = (int32_t)lrintf(lt.bucket_tiles * 100.0f);
   t->staging = NS_VARIANT_TABLE[lt.variant].ahead ? 2 : 1;
+  t->warps_per_cta = NS_VARIANT_TABLE[lt.variant].wpc;
 }
 
 dtb_status read_device_status(dtb_context ctx, const QueueHdr* hdr_dev, dtb_stats* st) {
@@ -770,21 +772,30 @@ DTB_API dtb_status dtb_context_create(int32_t device, dtb_context* out) {
   }
   static_assert(NS_VARIANT_TABLE[0].ctas == 2 && !NS_VARIANT_TABLE[0].ahead && NS_VARIANT_TABLE[1].ctas == 3 &&
                     NS_VARIANT_TABLE[2].ctas == 4 && NS_VARIANT_TABLE[3].ctas == 2 && NS_VARIANT_TABLE[3].ahead &&
-                    NS_VARIANT_TABLE[4].ctas == 3 && NS_VARIANT_TABLE[4].ahead,
+                    NS_VARIANT_TABLE[4].ctas == 3 && NS_VARIANT_TABLE[4].ahead && NS_VARIANT_TABLE[0].wpc == 4 &&
+                    NS_VARIANT_TABLE[1].wpc == 4 && NS_VARIANT_TABLE[2].wpc == 4 && NS_VARIANT_TABLE[3].wpc == 4 &&
+                    NS_VARIANT_TABLE[4].wpc == 4 && NS_VARIANT_TABLE[5].ctas == 6 && NS_VARIANT_TABLE[5].wpc == 2 &&
+                    NS_VARIANT_TABLE[6].ctas == 2 && NS_VARIANT_TABLE[6].wpc == 6 && NS_VARIANT_TABLE[7].ctas == 2 &&
+                    NS_VARIANT_TABLE[7].wpc == 8 && !NS_VARIANT_TABLE[5].ahead && !NS_VARIANT_TABLE[6].ahead &&
+                    !NS_VARIANT_TABLE[7].ahead,
                 "kernel instantiations below follow NS_VARIANT_TABLE");
   ctx->ns_fn[0] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 2>;
   ctx->ns_fn[1] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 3>;
   ctx->ns_fn[2] = (const void*)ggdt_persistent<MODE_NS, PERSIST_WPC, 4>;
   ctx->ns_fn[3] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 2>;
   ctx->ns_fn[4] = (const void*)ggdt_persistent_ahead<PERSIST_WPC, 3>;
+  ctx->ns_fn[5] = (const void*)ggdt_persistent<MODE_NS, 2, 6>;
+  ctx->ns_fn[6] = (const void*)ggdt_persistent<MODE_NS, 6, 2>;
+  ctx->ns_fn[7] = (const void*)ggdt_persistent<MODE_NS, 8, 2>;
   const void* kref = (const void*)ggdt_persistent<MODE_REF, PERSIST_WPC, REF_CTAS>;
   const void* kref_nofma = (const void*)ggdt_persistent<MODE_REF_NOFMA, PERSIST_WPC, REF_CTAS>;
   bool ok = true;
   for (int k = 0; k < NS_VARIANTS && ok; ++k) {
-    ctx->ns_smem[k] = NS_VARIANT_TABLE[k].ahead ? PERSIST_SMEM_AHEAD : PERSIST_SMEM;
+    const int wpc = NS_VARIANT_TABLE[k].wpc;
+    ctx->ns_smem[k] = wpc * (NS_VARIANT_TABLE[k].ahead ? sizeof(WarpSmemP) : sizeof(WarpSmem)) + 128;
     ok = cudaFuncSetAttribute(ctx->ns_fn[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->ns_smem[k]) ==
              cudaSuccess &&
-         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], PERSIST_WPC * 32,
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->ns_blocks_per_sm[k], ctx->ns_fn[k], wpc * 32,
                                                        ctx->ns_smem[k]) == cudaSuccess &&
          ctx->ns_blocks_per_sm[k] >= 1;
   }
@@ -865,10 +876,15 @@ DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t) 
   const NsVariant cur = NS_VARIANT_TABLE[nt.variant];
   const int ctas = t->ctas_per_sm != 0 ? t->ctas_per_sm : cur.ctas;
   const bool ahead = t->staging != 0 ? t->staging == 2 : cur.ahead;
+  // Warps per CTA: as given, else the current shape's if it goes with ctas_per_sm, else 4.
+  const int wpc = t->warps_per_cta != 0 ? t->warps_per_cta
+                  : ns_variant_of(ctas, ahead, cur.wpc) >= 0 ? cur.wpc
+                                                             : PERSIST_WPC;
   if (t->staging < 0 || t->staging > 2) return fail(ctx, DTB_ERR_INVALID_ARG, "staging must be 1 or 2");
-  const int variant = ns_variant_of(ctas, ahead);
+  const int variant = ns_variant_of(ctas, ahead, wpc);
   if (variant < 0)
-    return fail(ctx, DTB_ERR_INVALID_ARG, "ctas_per_sm must be 2, 3 or 4 (2 or 3 when the next tile is staged ahead)");
+    return fail(ctx, DTB_ERR_INVALID_ARG,
+                "(ctas_per_sm, warps_per_cta) must be (2|3|4, 4), (6, 2), (2, 6) or (2, 8); staging 2 needs (2|3, 4)");
   const int pct = t->grid_percent == 0 ? 100 : t->grid_percent;
   if (pct < 1 || pct > 100) return fail(ctx, DTB_ERR_INVALID_ARG, "grid_percent must be in [1, 100]");
   if (t->host_chunk_kpx < 0) return fail(ctx, DTB_ERR_INVALID_ARG, "host_chunk_kpx must be >= 0");

@@ -148,6 +148,12 @@ __device__ __forceinline__ uint64_t globaltimer() {
 
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 
+// Acquire-release fence at GPU scope: the release (data before a flag or counter update) and acquire (a flag
+// or counter read before the data) points of the tile visit and the queue.  Lighter than __threadfence()'s
+// sequentially consistent fence, which only the end-of-queue handshake (a store then a load of another word,
+// signal_done_warp) needs.
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -246,7 +252,7 @@ __device__ __forceinline__ uint32_t bucket_of(const Queue& q, float key, float i
 // Pushes one item into bucket b: pending += 1 before the item becomes visible.
 __device__ __forceinline__ void queue_push_to(const Queue& q, uint32_t b, uint32_t item) {
   atomicAdd(&q.hdr->pending.v, 1u);
-  __threadfence();
+  fence_acq_rel();
   slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
 }
 

@@ -23,19 +23,23 @@ constexpr size_t PERSIST_SMEM_AHEAD = PERSIST_WPC * sizeof(WarpSmemP) + 128;
 constexpr size_t ROUND_SMEM = ROUND_WPC * sizeof(WarpSmem) + 128;
 constexpr uint64_t DEFAULT_TIMEOUT_NS = 2000000000ull;
 constexpr int REF_CTAS = 3;  // resident CTAs per SM of the ref-mode tile kernels (168 registers)
-// ns-mode tile kernel variants: CTAs (of PERSIST_WPC warps) per SM (at most 255 / 168 / 128 registers for
-// 2 / 3 / 4) and whether a warp stages its next tile ahead (17 KB of shared memory a warp instead of 13 KB, so
-// at most 3 CTAs per SM).
+// ns-mode tile kernel variants: CTAs per SM, whether a warp stages its next tile ahead (17 KB of shared memory a
+// warp instead of 13 KB, so at most 3 CTAs of 4 warps per SM), and warps per CTA.  Registers per thread follow
+// the warps per SM: 8 -> 255, 12 -> 168, 16 -> 128.  The 12- and 16-warp shapes come in several CTA sizes
+// (2 x 6, 3 x 4, 6 x 2; 2 x 8, 4 x 4), which differ in how the SM's warps are grouped and scheduled only.
 struct NsVariant {
   int ctas;
   bool ahead;
+  int wpc;
 };
-constexpr int NS_VARIANTS = 5;
-constexpr NsVariant NS_VARIANT_TABLE[NS_VARIANTS] = {{2, false}, {3, false}, {4, false}, {2, true}, {3, true}};
-// Variant index of (ctas, ahead), or -1.
-inline int ns_variant_of(int ctas, bool ahead) {
+constexpr int NS_VARIANTS = 8;
+constexpr NsVariant NS_VARIANT_TABLE[NS_VARIANTS] = {{2, false, 4}, {3, false, 4}, {4, false, 4}, {2, true, 4},
+                                                     {3, true, 4},  {6, false, 2}, {2, false, 6}, {2, false, 8}};
+// Variant index of (ctas, ahead, warps per CTA), or -1.
+inline int ns_variant_of(int ctas, bool ahead, int wpc = PERSIST_WPC) {
   for (int k = 0; k < NS_VARIANTS; ++k)
-    if (NS_VARIANT_TABLE[k].ctas == ctas && NS_VARIANT_TABLE[k].ahead == ahead) return k;
+    if (NS_VARIANT_TABLE[k].ctas == ctas && NS_VARIANT_TABLE[k].ahead == ahead && NS_VARIANT_TABLE[k].wpc == wpc)
+      return k;
   return -1;
 }
 

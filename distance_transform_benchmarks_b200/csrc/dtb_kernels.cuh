@@ -54,7 +54,7 @@ struct QueueSched {
         const uint32_t kb = ld_volatile(&q.keys[tile]);
         pkey = kb == KEY_NONE ? 0.0f : __uint_as_float(kb);
       }
-      if (xor_bits & ST_VISITED) __threadfence();
+      if (xor_bits & ST_VISITED) fence_acq_rel();
     }
     __syncwarp();
     if (want) {
@@ -79,7 +79,7 @@ struct QueueSched {
       } else if (k > 1) {
         atomicAdd(&q.hdr->pending.v, k - 1u);
       }
-      __threadfence();
+      fence_acq_rel();
     }
     __syncwarp();
     if (push) {
@@ -309,7 +309,7 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
     if (lane < 4 && ((nexist >> lane) & 1u)) vis = (ld_volatile(&sch.states[nb_tile]) & ST_VISITED) != 0;
     nvis = __ballot_sync(~0u, vis);
   }
-  __threadfence();  // acquire: distances were written before the VISITED bits / the activation we saw
+  fence_acq_rel();  // acquire: distances were written before the VISITED bits / the activation we saw
 
   // Halo: column layout for top/bottom (lane = x), row layout for left/right (lane = y).
   float top = INF, bot = INF, lft = INF, rgt = INF;
@@ -541,7 +541,7 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
         if (y < vh) *reinterpret_cast<float*>(wb + (int64_t)y * dd.dist_pitch) = B[y * W_STRIDE + lane];
     }
   }
-  __threadfence();  // release: distances before activations and before the VISITED bit
+  fence_acq_rel();  // release: distances before activations and before the VISITED bit
   __syncwarp();
   sch.complete(tile, (first ? ST_VISITED : 0u) | (seed ? ST_SEED : 0u), lane < 4 && ((act >> lane) & 1u), nb_tile,
                act_key, inv_width);
@@ -615,7 +615,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
     nvis = __ballot_sync(~0u, vis);
     nexist = __ballot_sync(~0u, ex);
   }
-  __threadfence();
+  fence_acq_rel();
 
   // Halo rows / columns in shared memory, index = coordinate + 1 (corners appear in both).
   float* ht = sm.Wh;                // top row   (y0 - 1), x = -1..32
@@ -858,7 +858,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
         if (y < vh) *reinterpret_cast<float*>(wb + (int64_t)y * dd.dist_pitch) = T[y * S_STRIDE + lane];
     }
   }
-  __threadfence();
+  fence_acq_rel();
   __syncwarp();
   const bool want = lane < 8 && ((act >> lane) & 1u);
   const uint32_t item = want ? dd.tile_base + (uint32_t)((ty + ndy_l) * dd.tiles_x + tx + ndx_l) : 0u;

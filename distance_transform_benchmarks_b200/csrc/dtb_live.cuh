@@ -7,9 +7,11 @@
 // on the same stream, so a published entry's data is complete), idle warps of the running kernel notice the
 // published counter move, one of them claims the entry and turns it into work in the same tile queue the other
 // requests' tiles are in:
-//   new image   set-up jobs of 128 tiles: pass 1 writes the tile states (image slot, SEED from a scan of the
-//               mask tile), pass 2 -- once every pass-1 job of the image has ended, so that no activation can
-//               meet an uninitialised state -- queues the seed tiles;
+//   new image   set-up jobs, each a band of whole tile rows (about LIVE_JOB_TILES tiles): pass 1 moves rows
+//               the host staged packed into their pitched planes and writes the tile states (image slot, SEED
+//               from a scan of the mask tile), pass 2 -- once every pass-1 job of the image has ended, so that no
+//               activation can meet an uninitialised state and no visit a plane row not yet in place -- queues
+//               the seed tiles;
 //   seed edit   the claiming warp draws the disks into the resident mask and queues the tiles they touch; the
 //               tiles keep VISITED and their map, which is the warm start (added seeds only lower distances).
 // Each image slot counts its request's queued and running items; the warp whose completion brings the count to
@@ -20,7 +22,7 @@
 // Queue: one FIFO ring (the bucketed rings' ticket give-backs would move heads ahead of tails for as long as
 // the kernel lives); a waiting warp keeps its ticket while it admits an entry.  Termination: the kernel ends
 // when nothing is queued or running and the host asked it to stop, no request was claimed or completed for
-// `idle_ns`, or it has run for `life_ns` (after which it claims nothing new and drains); ending is one CAS of
+// `idle_us`, or it has run for `life_us` (after which it claims nothing new and drains); ending is one CAS of
 // the pending word from 0 to LIVE_EXIT, which an admission checks before it claims, so no entry is claimed by
 // a kernel that is ending.  Unclaimed entries are claimed by the next launch.  Every wait is bounded: a
 // no-progress watchdog (while work is pending) ends the kernel with an error code.
@@ -31,10 +33,10 @@
 namespace dtb {
 
 constexpr uint32_t LIVE_RING = 4096;          // request entries (power of two); at most LIVE_RING / 2 in flight
-constexpr uint32_t LIVE_JOB_TILES = 128;      // tiles per set-up job
+constexpr uint32_t LIVE_JOB_TILES = 64;       // tiles per set-up job (whole tile rows, at least one)
 constexpr uint32_t LIVE_JOB = 1u << 30;       // queue item: a set-up job (tile ids stay below 2^29)
 constexpr uint32_t LIVE_JOB_PASS2 = 1u << 29; // set-up job, second pass (queue the seed tiles)
-constexpr int LIVE_CHUNK_BITS = 15;           // set-up jobs per pass < 32768 (4M tiles per image)
+constexpr int LIVE_CHUNK_BITS = 15;           // set-up jobs per pass < 32768 (tile rows < 32768)
 constexpr int LIVE_SLOT_BITS = 14;            // image slots < 16384
 constexpr uint32_t LIVE_MAX_SLOTS = 1u << LIVE_SLOT_BITS;
 constexpr uint32_t LIVE_MAX_TILES = 1u << 29; // tile ids of the live tile space
@@ -49,9 +51,10 @@ enum : uint32_t { LIVE_NEW = 0u, LIVE_EDIT = 1u };
 struct alignas(32) LiveEntry {
   uint32_t kind;     // LIVE_NEW / LIVE_EDIT
   uint32_t slot;     // image slot: descriptor, tensor maps and counters
-  uint32_t n_disks;  // edit: disks (cx, cy, r int32 triples) at disks[disk_idx ..]
+  uint32_t n_disks;  // edit: disks (cx, cy, r, 0: 16-byte records) at disks[4 * disk_idx ..]
   uint32_t disk_idx;
-  uint32_t pad[4];
+  uint32_t stage;    // new image: LIVE_STAGE_* flags
+  uint32_t pad[3];
 };
 
 // Host <-> kernel words in device memory, kept across launches (the queue header is reset per launch).
@@ -62,15 +65,26 @@ struct LiveHdr {
   Line inject;      // failure self-test: the next claimed request counts one item that never runs
   Line last_busy;   // low 32 bits of the globaltimer (us) of the last claim or completion
   Line watch_ms;    // no-progress limit of the watchdog (ms)
+  Line end_reason;  // why the last launch ended: LIVE_END_STOP / _IDLE / _LIFE (0: an error, or still running)
 };
+constexpr uint32_t LIVE_END_STOP = 1u, LIVE_END_IDLE = 2u, LIVE_END_LIFE = 3u;
 
 // Per image slot.
 struct LiveSlot {
   uint32_t pending;     // set-up jobs and tiles of the slot's request queued or running, + 1 while admitting
   uint32_t entry;       // entry index of that request
   uint32_t setup_left;  // pass-1 set-up jobs not yet ended
-  uint32_t pad;
+  uint32_t stage;       // new image: LIVE_STAGE_* planes staged packed in its distance plane
 };
+
+// A new image's planes whose rows need a new pitch are copied in packed, into the image's own distance plane
+// (not written before the set-up ends; at least (channels + 1) bytes a pixel): the image at its start, the mask
+// after it, 16-byte aligned.  Pass-1 set-up jobs move the rows into place.
+constexpr uint32_t LIVE_STAGE_IMG = 1u, LIVE_STAGE_MASK = 2u;
+constexpr uint64_t LIVE_STAGE_SLACK = 64;  // bytes the staging leaves free at the end of the distance plane
+__host__ __device__ __forceinline__ uint64_t live_stage_mask_offset(uint32_t rb, uint32_t h) {
+  return ((uint64_t)rb * h + 15u) & ~uint64_t(15);
+}
 
 struct LiveArgs {
   Queue q;                    // one FIFO ring; total_tiles = size of the tile space
@@ -98,6 +112,11 @@ __device__ __forceinline__ ImgDesc load_desc(const ImgDesc* p) {
 #pragma unroll
   for (int k = 0; k < (int)(sizeof(ImgDesc) / 16); ++k) o[k] = __ldcg(s + k);
   return d;
+}
+
+// Tile rows of one set-up job: whole tile rows, about LIVE_JOB_TILES tiles.
+__device__ __forceinline__ uint32_t live_band(const ImgDesc& dd) {
+  return max(1u, LIVE_JOB_TILES / (uint32_t)max(dd.tiles_x, 1));
 }
 
 // Item pushes of the live kernel: the caller has already counted them in `pending` (global and slot).
@@ -241,8 +260,10 @@ __device__ bool live_admit(const LiveArgs& a, uint32_t t_start) {
   }
   const uint32_t tiles = (uint32_t)dd.tiles_x * (uint32_t)dd.tiles_y;
   if (kind == LIVE_NEW) {
-    const uint32_t njobs = (tiles + LIVE_JOB_TILES - 1u) / LIVE_JOB_TILES;
+    const uint32_t band = live_band(dd);
+    const uint32_t njobs = tiles ? ((uint32_t)dd.tiles_y + band - 1u) / band : 0u;
     if (lane == 0 && njobs) {
+      ls->stage = __ldcg(&pe->stage);
       ls->setup_left = njobs;
       if (q.wacc) { q.wacc[2 * slot] = 0.0f; q.wacc[2 * slot + 1] = 0.0f; }
       atomicAdd(&q.hdr->pending.v, njobs);
@@ -255,7 +276,8 @@ __device__ bool live_admit(const LiveArgs& a, uint32_t t_start) {
     // Draw the disks into the resident mask (the same pixels as serve_draw_disks).
     uint8_t* mask = const_cast<uint8_t*>(dd.mask);
     for (uint32_t k = 0; k < nd; ++k) {
-      const int cx = __ldcg(a.disks + 3 * (di + k)), cy = __ldcg(a.disks + 3 * (di + k) + 1), r = __ldcg(a.disks + 3 * (di + k) + 2);
+      const int4 dk = __ldcg(reinterpret_cast<const int4*>(a.disks) + (di + k));
+      const int cx = dk.x, cy = dk.y, r = dk.z;
       const int xa = max(0, cx - r), xb = min(dd.width - 1, cx + r), ya = max(0, cy - r), yb = min(dd.height - 1, cy + r);
       if (xa > xb || ya > yb) continue;
       const int bw = xb - xa + 1, cnt = bw * (yb - ya + 1);
@@ -271,7 +293,8 @@ __device__ bool live_admit(const LiveArgs& a, uint32_t t_start) {
     // Queue the tiles the disks touch (as serve_seed_tiles); the image has no other request in flight, so every
     // tile is idle and VISITED.
     for (uint32_t k = 0; k < nd; ++k) {
-      const int cx = __ldcg(a.disks + 3 * (di + k)), cy = __ldcg(a.disks + 3 * (di + k) + 1), r = __ldcg(a.disks + 3 * (di + k) + 2);
+      const int4 dk = __ldcg(reinterpret_cast<const int4*>(a.disks) + (di + k));
+      const int cx = dk.x, cy = dk.y, r = dk.z;
       const int xa = max(0, cx - r), xb = min(dd.width - 1, cx + r), ya = max(0, cy - r), yb = min(dd.height - 1, cy + r);
       if (xa > xb || ya > yb) continue;
       const int txa = xa / TILE, txb = xb / TILE, tya = ya / TILE, tyb = yb / TILE;
@@ -304,7 +327,41 @@ __device__ bool live_admit(const LiveArgs& a, uint32_t t_start) {
   return true;
 }
 
-// One set-up job of a new image (whole warp).
+// Rows [y0, y1) of a plane copied packed (row r at src + r * rb) into its pitched place (row r at dst + r *
+// pitch), as 16-byte chunks of the destination: the destination rows are 128-byte aligned, the packed source
+// rows only byte aligned, so a chunk is five aligned 4-byte source words funnel-shifted by the row's byte
+// offset (the same for every chunk of a row).  Each lane keeps four chunks' loads in flight.  A row's last
+// chunk may carry up to 15 bytes past the row into the pitch padding, and the loads may read up to 19 bytes past
+// the packed data: the host leaves LIVE_STAGE_SLACK bytes free.  The source was written by a host copy into
+// memory whose earlier contents this SM may have cached, so the loads go through L2.
+__device__ __forceinline__ void live_repitch(const uint8_t* src, uint8_t* dst, int64_t pitch, uint32_t rb, int y0, int y1) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t chunks = (rb + 15u) / 16u;
+  for (int y = y0; y < y1; ++y) {
+    const uintptr_t sa = reinterpret_cast<uintptr_t>(src) + (uintptr_t)y * rb;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(sa & ~uintptr_t(3));
+    const uint32_t sh = (uint32_t)(sa & 3u) * 8u;
+    uint4* d = reinterpret_cast<uint4*>(dst + (int64_t)y * pitch);
+    for (uint32_t c0 = (uint32_t)lane; c0 < chunks; c0 += 32u * 4u) {
+      uint32_t v[4][5];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t c = c0 + 32u * (uint32_t)u;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) v[u][j] = c < chunks ? __ldcg(w + 4u * c + (uint32_t)j) : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t c = c0 + 32u * (uint32_t)u;
+        if (c < chunks)
+          d[c] = make_uint4(__funnelshift_r(v[u][0], v[u][1], sh), __funnelshift_r(v[u][1], v[u][2], sh),
+                            __funnelshift_r(v[u][2], v[u][3], sh), __funnelshift_r(v[u][3], v[u][4], sh));
+      }
+    }
+  }
+}
+
+// One set-up job of a new image (whole warp): a band of whole tile rows.
 __device__ void live_job(const LiveArgs& a, uint32_t item) {
   const int lane = threadIdx.x & 31;
   const Queue& q = a.q;
@@ -312,35 +369,63 @@ __device__ void live_job(const LiveArgs& a, uint32_t item) {
   const uint32_t chunk = item & ((1u << LIVE_CHUNK_BITS) - 1u);
   const bool pass2 = (item & LIVE_JOB_PASS2) != 0u;
   const ImgDesc dd = load_desc(a.descs + slot);
-  const uint32_t tiles = (uint32_t)dd.tiles_x * (uint32_t)dd.tiles_y;
-  const uint32_t t0 = chunk * LIVE_JOB_TILES, t1 = min(t0 + LIVE_JOB_TILES, tiles);
+  const uint32_t band = live_band(dd);
+  const uint32_t ty0 = chunk * band, ty1 = min(ty0 + band, (uint32_t)dd.tiles_y);
+  const uint32_t t0 = ty0 * (uint32_t)dd.tiles_x, t1 = ty1 * (uint32_t)dd.tiles_x;
   LiveSlot* ls = a.slots + slot;
   if (!pass2) {
-    // States of the chunk: the slot, and SEED where the mask tile holds a seed (lane = row of the tile).
-    for (uint32_t t = t0; t < t1; ++t) {
-      const int x0 = (int)(t % (uint32_t)dd.tiles_x) * TILE, y0 = (int)(t / (uint32_t)dd.tiles_x) * TILE;
-      const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
-      bool nz = false;
-      if (lane < vh) {
-        const uint8_t* row = dd.mask + (int64_t)(y0 + lane) * dd.mask_pitch + x0;
-        if (vw == TILE && (reinterpret_cast<uintptr_t>(row) & 15u) == 0) {
-          const uint4 u = __ldcg(reinterpret_cast<const uint4*>(row));
-          const uint4 v = __ldcg(reinterpret_cast<const uint4*>(row) + 1);
-          nz = (u.x | u.y | u.z | u.w | v.x | v.y | v.z | v.w) != 0u;
-        } else {
-          for (int c = 0; c < vw; ++c) nz |= __ldcg(row + c) != 0;
+    // Rows of the band staged packed in the distance plane move into their pitched planes first (the host
+    // copied them as one 1-D copy each: a copy that changes the pitch runs at a fraction of the link's rate).
+    const uint32_t stage = ld_volatile(&ls->stage);
+    if (stage) {
+      const int y0 = (int)ty0 * TILE, y1 = min((int)ty1 * TILE, dd.height);
+      const uint32_t rb = (uint32_t)dd.width * (uint32_t)dd.channels;
+      const uint8_t* st = reinterpret_cast<const uint8_t*>(dd.dist);
+      if (stage & LIVE_STAGE_IMG) live_repitch(st, const_cast<uint8_t*>(dd.img), dd.img_pitch, rb, y0, y1);
+      if (stage & LIVE_STAGE_MASK)
+        live_repitch(st + ((stage & LIVE_STAGE_IMG) ? live_stage_mask_offset(rb, (uint32_t)dd.height) : 0),
+                     const_cast<uint8_t*>(dd.mask), dd.mask_pitch, (uint32_t)dd.width, y0, y1);
+      // The planes are read by bulk copies (async proxy) in the visits.
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      __threadfence();
+      __syncwarp();
+    }
+    // States of the band: the slot, and SEED where the mask tile holds a seed (lane = row of the tile; four
+    // tiles' loads in flight at once).
+    for (uint32_t tb = t0; tb < t1; tb += 4u) {
+      bool nz[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t t = tb + (uint32_t)u;
+        nz[u] = false;
+        if (t < t1) {
+          const int x0 = (int)(t % (uint32_t)dd.tiles_x) * TILE, y0 = (int)(t / (uint32_t)dd.tiles_x) * TILE;
+          const int vw = min(TILE, dd.width - x0), vh = min(TILE, dd.height - y0);
+          if (lane < vh) {
+            const uint8_t* row = dd.mask + (int64_t)(y0 + lane) * dd.mask_pitch + x0;
+            if (vw == TILE && (reinterpret_cast<uintptr_t>(row) & 15u) == 0) {
+              const uint4 p = __ldcg(reinterpret_cast<const uint4*>(row));
+              const uint4 r = __ldcg(reinterpret_cast<const uint4*>(row) + 1);
+              nz[u] = (p.x | p.y | p.z | p.w | r.x | r.y | r.z | r.w) != 0u;
+            } else {
+              for (int c = 0; c < vw; ++c) nz[u] |= __ldcg(row + c) != 0;
+            }
+          }
         }
       }
-      nz = __any_sync(~0u, nz);
-      if (lane == 0) a.states[dd.tile_base + t] = (slot << ST_IMG_SHIFT) | (nz ? ST_SEED : 0u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool any = __any_sync(~0u, nz[u]);
+        if (lane == 0 && tb + (uint32_t)u < t1) a.states[dd.tile_base + tb + u] = (slot << ST_IMG_SHIFT) | (any ? ST_SEED : 0u);
+      }
     }
     __threadfence();
     __syncwarp();
     uint32_t all = 0;
     if (lane == 0) all = atomicSub(&ls->setup_left, 1u) == 1u ? 1u : 0u;
     if (__shfl_sync(~0u, all, 0)) {
-      // Every state of the image is written: queue the second pass.
-      const uint32_t njobs = (tiles + LIVE_JOB_TILES - 1u) / LIVE_JOB_TILES;
+      // Every state and plane row of the image is written: queue the second pass.
+      const uint32_t njobs = ((uint32_t)dd.tiles_y + band - 1u) / band;
       if (lane == 0) {
         atomicAdd(&q.hdr->pending.v, njobs);
         atomicAdd(&ls->pending, njobs);
@@ -351,7 +436,7 @@ __device__ void live_job(const LiveArgs& a, uint32_t item) {
         live_push(q, LIVE_JOB | LIVE_JOB_PASS2 | (slot << LIVE_CHUNK_BITS) | j);
     }
   } else {
-    // Queue the seed tiles of the chunk.  A tile an activation has queued or visited meanwhile is left alone
+    // Queue the seed tiles of the band.  A tile an activation has queued or visited meanwhile is left alone
     // (its visit applies or applied the seeds); a visited one queued again only costs a converged visit.
     for (uint32_t tb = t0; tb < t1; tb += 32u) {
       const uint32_t t = tb + (uint32_t)lane;
@@ -401,9 +486,16 @@ __device__ __forceinline__ uint32_t live_take(const LiveArgs& a, uint32_t h, Pop
       if (pend == 0u) {
         w.t_prog = now;  // nothing to watch while idle
         const uint32_t tn = (uint32_t)(now / 1000ull);
-        const bool idle = tn - ld_volatile(&a.lh->last_busy.v) > a.idle_us && tn - t_start > a.idle_us;
-        if ((ld_volatile(&a.lh->stop.v) | (idle ? 1u : 0u)) || tn - t_start >= a.life_us) {
-          if (atomicCAS(&q.hdr->pending.v, 0u, LIVE_EXIT) == 0u) return LIVE_END;
+        // Signed differences: another warp may have stamped last_busy after this warp read the clock.
+        const bool idle = (int32_t)(tn - ld_volatile(&a.lh->last_busy.v)) > (int32_t)a.idle_us &&
+                          (int32_t)(tn - t_start) > (int32_t)a.idle_us;
+        const uint32_t why = ld_volatile(&a.lh->stop.v) ? LIVE_END_STOP
+                             : idle                     ? LIVE_END_IDLE
+                             : (int32_t)(tn - t_start) >= (int32_t)a.life_us ? LIVE_END_LIFE
+                                                         : 0u;
+        if (why && atomicCAS(&q.hdr->pending.v, 0u, LIVE_EXIT) == 0u) {
+          atomicExch(&a.lh->end_reason.v, why);
+          return LIVE_END;
         }
         continue;
       }
@@ -474,9 +566,9 @@ __global__ void __launch_bounds__(WPC * 32, MINB) ggdt_live(LiveArgs a) {
     old = __shfl_sync(~0u, old, 0);
     const uint32_t slot = old >> ST_IMG_SHIFT;
     const ImgDesc dd = load_desc(a.descs + slot);
-    if (old & ST_SEED) {  // an edit drew this tile's seeds by generic stores; the visit reads them by bulk copy
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-    }
+    // A first visit reads planes that a set-up job may have moved into place, and a seed visit a mask an edit
+    // drew into, by generic stores; the visit reads them by bulk copy (async proxy).
+    if ((old & ST_SEED) || !(old & ST_VISITED)) asm volatile("fence.proxy.async.global;" ::: "memory");
     uint32_t nph, nact;
     visit_ns<false>(dd, a.tmaps + 2 * slot, a.tmaps + 2 * slot + 1, it, old, visit_bufs(sm, parity), sch, &nph, &nact);
     count_visit(ws, a.q, nph, nact);

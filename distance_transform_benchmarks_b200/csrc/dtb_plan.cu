@@ -65,7 +65,7 @@ bool aligned16(const dtb_image* im) {
 struct CacheEntry {
   std::string gpu;
   uint64_t images = 0, tiles = 0;
-  int ctas = 0, staging = 0, grid = 0, buckets = 0, width_pct = 0;
+  int ctas = 0, staging = 0, grid = 0, buckets = 0, width_pct = 0, wpc = 4;  // wpc: 4 in caches written without it
   double ms = 0.0;
 };
 
@@ -106,6 +106,7 @@ std::vector<CacheEntry> parse_cache(const std::string& text) {
       else if (key == "tiles_pow2") c.tiles = std::strtoull(val.c_str(), nullptr, 10);
       else if (key == "ctas_per_sm") c.ctas = std::atoi(val.c_str());
       else if (key == "staging") c.staging = std::atoi(val.c_str());
+      else if (key == "warps_per_cta") c.wpc = std::atoi(val.c_str());
       else if (key == "grid_percent") c.grid = std::atoi(val.c_str());
       else if (key == "queue_buckets") c.buckets = std::atoi(val.c_str());
       else if (key == "bucket_width_pct") c.width_pct = std::atoi(val.c_str());
@@ -140,7 +141,7 @@ dtb_status load_tuning_cache(dtb_context ctx) {
   if (!read_file(ctx->tune_cache_path, &text)) return DTB_OK;  // no cache yet
   for (const CacheEntry& c : parse_cache(text)) {
     if (c.gpu != ctx->gpu_name) continue;
-    const int v = ns_variant_of(c.ctas, c.staging == 2);
+    const int v = ns_variant_of(c.ctas, c.staging == 2, c.wpc);
     if (v < 0 || c.grid < 1 || c.grid > 100 || !valid_policy(c.buckets, (float)c.width_pct / 100.0f)) continue;
     LaunchTuning t;
     t.variant = v;
@@ -164,6 +165,7 @@ dtb_status save_tuning_cache(dtb_context ctx, uint64_t key, const LaunchTuning& 
   n.tiles = key & 0xFFFFFFFFull;
   n.ctas = NS_VARIANT_TABLE[t.variant].ctas;
   n.staging = NS_VARIANT_TABLE[t.variant].ahead ? 2 : 1;
+  n.wpc = NS_VARIANT_TABLE[t.variant].wpc;
   n.grid = t.grid_percent;
   n.buckets = t.buckets;
   n.width_pct = (int)lrintf(t.bucket_tiles * 100.0f);
@@ -183,9 +185,9 @@ dtb_status save_tuning_cache(dtb_context ctx, uint64_t key, const LaunchTuning& 
     const CacheEntry& c = entries[i];
     std::fprintf(f,
                  "%s\n  {\"gpu\": \"%s\", \"images_pow2\": %llu, \"tiles_pow2\": %llu, \"ctas_per_sm\": %d, \"staging\": %d, "
-                 "\"grid_percent\": %d, \"queue_buckets\": %d, \"bucket_width_pct\": %d, \"ms\": %.4f}",
+                 "\"warps_per_cta\": %d, \"grid_percent\": %d, \"queue_buckets\": %d, \"bucket_width_pct\": %d, \"ms\": %.4f}",
                  i ? "," : "", c.gpu.c_str(), (unsigned long long)c.images, (unsigned long long)c.tiles, c.ctas, c.staging,
-                 c.grid, c.buckets, c.width_pct, c.ms);
+                 c.wpc, c.grid, c.buckets, c.width_pct, c.ms);
   }
   std::fprintf(f, "\n]}\n");
   const bool ok = std::fclose(f) == 0 && std::rename(tmp.c_str(), ctx->tune_cache_path.c_str()) == 0;
@@ -307,9 +309,9 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
       best = t;
     }
   };
-  // Coordinate search: (1) kernel variant x grid share under the current queue policy; (2) queue policy
-  // (FIFO; 8 or 16 buckets of 1/4, 1/2 or 1 tile-width) under the best launch; (3) the variants again under the
-  // best policy.
+  // Coordinate search: (1) kernel variant (CTAs per SM x warps per CTA x staging) x grid share under the current
+  // queue policy; (2) queue policy (FIFO; 8 or 16 buckets of 1/4, 1/2 or 1 tile-width) under the best launch;
+  // (3) the variants again under the best policy.
   static const int kPercent[3] = {100, 75, 50};
   const LaunchTuning start = p->tuning;
   for (int v = 0; v < NS_VARIANTS; ++v)

@@ -731,6 +731,7 @@ constexpr uint32_t LIVE_WATCH_MS = 2000;       // no-progress limit of the live 
 constexpr uint32_t LIVE_LIFE_US = 4000000;     // a launch claims new requests for this long, then drains and ends
 constexpr uint32_t LIVE_IDLE_US = 20000;       // default idle time after which a launch ends
 constexpr uint32_t LIVE_DISK_CAP = 1u << 20;   // disks of edits in flight
+constexpr size_t LIVE_DISK_BYTES = 16;         // a disk record (cx, cy, r, 0) in the pool
 constexpr int LIVE_CTAS = 3;                   // CTAs of PERSIST_WPC warps per SM (the 168-register launch)
 
 // A published request.
@@ -808,7 +809,7 @@ dtb_status live_create(dtb_server s, uint32_t idle_us) {
   L->grid = (uint32_t)ctx->num_sms * (uint32_t)std::min(per_sm, LIVE_CTAS);
   const uint32_t workers = L->grid * PERSIST_WPC;
   // Ring: items in flight (tiles of the requests in flight, their set-up jobs) plus waiting workers.
-  const uint64_t items = (uint64_t)s->max_tiles + 2ull * (s->max_tiles / LIVE_JOB_TILES + (uint64_t)s->max_reqs) +
+  const uint64_t items = (uint64_t)s->max_tiles + 2ull * (s->max_tiles + (uint64_t)s->max_reqs) +
                          workers + 64;
   uint32_t cap = 1;
   while (cap < 2 * items && cap < (1u << 30)) cap <<= 1;
@@ -822,7 +823,7 @@ dtb_status live_create(dtb_server s, uint32_t idle_us) {
   const size_t o_tmap = off;    off = align_up(off + 2 * sizeof(CUtensorMap) * L->nslots, 256);
   const size_t o_slots = off;   off = align_up(off + sizeof(LiveSlot) * L->nslots, 256);
   const size_t o_ent = off;     off = align_up(off + sizeof(LiveEntry) * LIVE_RING, 256);
-  const size_t o_disks = off;   off = align_up(off + 12ull * LIVE_DISK_CAP, 256);
+  const size_t o_disks = off;   off = align_up(off + LIVE_DISK_BYTES * LIVE_DISK_CAP, 256);
   if (cudaMalloc((void**)&L->dmem, off) != cudaSuccess) {
     cudaGetLastError();
     return fail(ctx, DTB_ERR_OUT_OF_MEMORY, "serve (live): cudaMalloc of %zu bytes failed", off);
@@ -836,7 +837,7 @@ dtb_status live_create(dtb_server s, uint32_t idle_us) {
   L->slots = reinterpret_cast<LiveSlot*>(L->dmem + o_slots);
   L->entries = reinterpret_cast<LiveEntry*>(L->dmem + o_ent);
   L->disks = reinterpret_cast<int32_t*>(L->dmem + o_disks);
-  const size_t hbytes = LIVE_STAGE * LIVE_RING + 12ull * LIVE_DISK_CAP + 256;
+  const size_t hbytes = LIVE_STAGE * LIVE_RING + LIVE_DISK_BYTES * LIVE_DISK_CAP + 256;
   if (cudaHostAlloc((void**)&L->hstage, hbytes, cudaHostAllocDefault) != cudaSuccess ||
       cudaHostAlloc((void**)&L->hdone, 4ull * LIVE_RING, cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer((void**)&L->ddone, L->hdone, 0) != cudaSuccess ||
@@ -847,11 +848,11 @@ dtb_status live_create(dtb_server s, uint32_t idle_us) {
   std::memset(L->hstage, 0, hbytes);
   std::memset(L->hdone, 0, 4ull * LIVE_RING);
   L->hdisks = reinterpret_cast<int32_t*>(L->hstage + LIVE_STAGE * LIVE_RING);
-  L->hwords = reinterpret_cast<uint32_t*>(L->hstage + LIVE_STAGE * LIVE_RING + 12ull * LIVE_DISK_CAP);
+  L->hwords = reinterpret_cast<uint32_t*>(L->hstage + LIVE_STAGE * LIVE_RING + LIVE_DISK_BYTES * LIVE_DISK_CAP);
   L->hwords[0] = 1u;
   L->hwords[1] = LIVE_WATCH_MS;
   L->tiles.reset(4ull * L->tile_cap);
-  L->diskpool.reset(12ull * LIVE_DISK_CAP);
+  L->diskpool.reset(LIVE_DISK_BYTES * LIVE_DISK_CAP);
   for (int32_t k = (int32_t)L->nslots - 1; k >= 0; --k) L->free_slots.push_back(k);
   // Everything starts at zero (states, counters, entries); the watchdog limit is set once.
   DTB_CUDA(ctx, cudaMemsetAsync(L->dmem, 0, off, s->s_run));
@@ -927,7 +928,7 @@ std::vector<LiveFlight> live_admit_host(dtb_server s) {
         continue;
       }
       LiveFlight f;
-      f.disk_bytes = 12 * (q.disks.size() / 3);
+      f.disk_bytes = LIVE_DISK_BYTES * (q.disks.size() / 3);
       if (f.disk_bytes) {
         size_t doff = 0;
         if (!L->diskpool.alloc(f.disk_bytes, &doff)) {
@@ -953,7 +954,7 @@ std::vector<LiveFlight> live_admit_host(dtb_server s) {
       continue;
     }
     const uint64_t t = tiles_of(q.r.img.width, q.r.img.height);
-    if (t > s->max_tiles || t > (uint64_t)LIVE_JOB_TILES << LIVE_CHUNK_BITS) {
+    if (t > s->max_tiles || (uint64_t)(q.r.img.height + 31) / 32 >= (1ull << LIVE_CHUNK_BITS)) {
       complete(s, q, DTB_ERR_CAPACITY, now);
       continue;
     }
@@ -1024,12 +1025,28 @@ dtb_status live_publish(dtb_server s, LiveFlight& f, const Resident& r) {
     ent->kind = LIVE_NEW;
     const size_t rb = (size_t)r.W * r.C;
     if (r.W > 0 && r.H > 0) {
-      if ((size_t)q.img.pitch == rb && (size_t)r.img_pitch == rb)
+      // Planes whose rows need a new pitch go in packed, as one 1-D copy, into the image's distance plane, and the
+      // kernel's set-up jobs move the rows into place (a 2-D copy that changes the pitch runs at 12-30 GB/s
+      // against 47-54 GB/s for a 1-D copy); if the host rows are padded themselves, or the staging does not fit,
+      // a 2-D copy goes straight into place.
+      bool st_img = (size_t)r.img_pitch != rb && (size_t)q.img.pitch == rb;
+      bool st_mask = r.mask_pitch != r.W && q.mask.pitch == r.W;
+      const uint64_t o_mask_st = st_img ? live_stage_mask_offset((uint32_t)rb, (uint32_t)r.H) : 0;
+      const uint64_t need = o_mask_st + (st_mask ? (uint64_t)r.W * r.H : 0) + LIVE_STAGE_SLACK;
+      if (need > (uint64_t)r.dist_pitch * r.H) st_img = st_mask = false;
+      uint8_t* stage = base + r.o_dist;
+      ent->stage = (st_img ? LIVE_STAGE_IMG : 0u) | (st_mask ? LIVE_STAGE_MASK : 0u);
+      if (st_img)
+        DTB_CUDA(ctx, cudaMemcpyAsync(stage, q.img.buffer, rb * r.H, cudaMemcpyHostToDevice, st));
+      else if ((size_t)q.img.pitch == rb && (size_t)r.img_pitch == rb)
         DTB_CUDA(ctx, cudaMemcpyAsync(base + r.o_img, q.img.buffer, rb * r.H, cudaMemcpyHostToDevice, st));
       else
         DTB_CUDA(ctx, cudaMemcpy2DAsync(base + r.o_img, r.img_pitch, q.img.buffer, q.img.pitch, rb, r.H,
                                         cudaMemcpyHostToDevice, st));
-      if (q.mask.pitch == r.W && r.mask_pitch == r.W)
+      if (st_mask)
+        DTB_CUDA(ctx, cudaMemcpyAsync(stage + (st_img ? o_mask_st : 0), q.mask.buffer, (size_t)r.W * r.H,
+                                      cudaMemcpyHostToDevice, st));
+      else if (q.mask.pitch == r.W && r.mask_pitch == r.W)
         DTB_CUDA(ctx, cudaMemcpyAsync(base + r.o_mask, q.mask.buffer, (size_t)r.W * r.H, cudaMemcpyHostToDevice, st));
       else
         DTB_CUDA(ctx, cudaMemcpy2DAsync(base + r.o_mask, r.mask_pitch, q.mask.buffer, q.mask.pitch, r.W, r.H,
@@ -1060,10 +1077,17 @@ dtb_status live_publish(dtb_server s, LiveFlight& f, const Resident& r) {
     const size_t nd = f.q.disks.size() / 3;
     ent->n_disks = (uint32_t)nd;
     if (nd) {
-      ent->disk_idx = (uint32_t)(f.disk_off / 12);
-      std::memcpy(reinterpret_cast<uint8_t*>(L->hdisks) + f.disk_off, f.q.disks.data(), 12 * nd);
-      DTB_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<uint8_t*>(L->disks) + f.disk_off,
-                                    reinterpret_cast<uint8_t*>(L->hdisks) + f.disk_off, 12 * nd, cudaMemcpyHostToDevice, st));
+      // 16-byte records: pool offsets (multiples of the arena's 256-byte granule) are whole records.
+      ent->disk_idx = (uint32_t)(f.disk_off / LIVE_DISK_BYTES);
+      int32_t* hd = L->hdisks + f.disk_off / 4;
+      for (size_t k = 0; k < nd; ++k) {
+        hd[4 * k] = f.q.disks[3 * k];
+        hd[4 * k + 1] = f.q.disks[3 * k + 1];
+        hd[4 * k + 2] = f.q.disks[3 * k + 2];
+        hd[4 * k + 3] = 0;
+      }
+      DTB_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<uint8_t*>(L->disks) + f.disk_off, hd, LIVE_DISK_BYTES * nd,
+                                    cudaMemcpyHostToDevice, st));
     }
   }
   // dtb_debug_inject_queue_stall on the server's context: the next request the kernel claims counts one item
@@ -1090,6 +1114,7 @@ dtb_status live_launch(dtb_server s) {
   cudaStream_t st = s->s_run;
   DTB_CUDA(ctx, cudaMemsetAsync(L->qhdr, 0, sizeof(QueueHdr), st));
   DTB_CUDA(ctx, cudaMemsetAsync(L->ring, 0, 4ull * L->ring_cap, st));
+  DTB_CUDA(ctx, cudaMemsetAsync(&L->lh->end_reason.v, 0, 4, st));
   LiveArgs a{};
   a.q.hdr = L->qhdr;
   a.q.ring = L->ring;
@@ -1150,6 +1175,10 @@ void live_after_kernel(dtb_server s) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->st.tile_visits += h.progress.v;
   L->claimed_seen = lhh.claimed.v;
+  if (status != DTB_OK) s->st.live_ended_error += 1;
+  else if (lhh.end_reason.v == LIVE_END_IDLE) s->st.live_ended_idle += 1;
+  else if (lhh.end_reason.v == LIVE_END_LIFE) s->st.live_ended_lifetime += 1;
+  else if (lhh.end_reason.v == LIVE_END_STOP) s->st.live_ended_stop += 1;
   if (status == DTB_OK) return;
   // Requests claimed by the failed launch (entries below `claimed`) whose completion word is not written fail.
   const auto now = Clock::now();

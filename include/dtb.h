@@ -97,7 +97,9 @@ DTB_API dtb_status dtb_sync(dtb_context ctx, void* stream);
  * The reference fixes its choices at build time: 64 priority levels from seed distances
  * (dt/src/task_queue.cuh:23, dt/src/block_priority.cu:71-155) and 4 blocks of one warp per SM
  * (dt/src/generalised_distance_transform_task.cu:184).  0 keeps a field's current value.
- * ctas_per_sm: resident CTAs of 4 warps per SM, 2, 3 or 4 (registers per thread 255 / 168 / 128);
+ * ctas_per_sm and warps_per_cta: the launch shape, one warp per 32 x 32 tile visit; (2, 4), (3, 4), (4, 4),
+ * (6, 2), (2, 6) or (2, 8) -- 8, 12 or 16 warps per SM, registers per thread 255 / 168 / 128 (with only
+ * ctas_per_sm given, warps_per_cta stays if it fits, else becomes 4);
  * grid_percent: share of the co-resident CTAs launched, 1..100 (fewer workers re-visit fewer tiles on
  * narrow fronts); host_chunk_kpx: pixels (in units of 1024) per chunk of the pipeline that serves batches in
  * host memory (host-to-device copies, tile runs on two alternating compute lanes and device-to-host copies of
@@ -113,6 +115,7 @@ typedef struct dtb_tuning {
   int32_t queue_buckets;
   int32_t bucket_width_pct;
   int32_t staging;
+  int32_t warps_per_cta;
 } dtb_tuning;
 DTB_API dtb_status dtb_context_set_tuning(dtb_context ctx, const dtb_tuning* t);
 DTB_API dtb_status dtb_context_get_tuning(dtb_context ctx, dtb_tuning* t);
@@ -235,6 +238,9 @@ typedef struct dtb_serve_stats {
    * preparation; sum and maximum over requests). */
   double host_prep_ms, copy_in_ms, kernel_ms, copy_out_ms, queue_wait_ms, queue_wait_max_ms;
   int64_t waves_split;        /* waves closed by a per-wave limit (tiles, staging, disks) with requests left over */
+  /* Live engine: launches of the live kernel that ended idle (live_idle_us without work), at the end of their
+   * lifetime (4 s, then drained), on a device error, or on dtb_serve_destroy. */
+  int64_t live_ended_idle, live_ended_lifetime, live_ended_error, live_ended_stop;
 } dtb_serve_stats;
 typedef struct dtb_server_s* dtb_server;
 DTB_API dtb_status dtb_serve_create(dtb_context ctx, const dtb_serve_config* cfg, dtb_server* out);

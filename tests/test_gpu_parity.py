@@ -379,7 +379,7 @@ def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
         for k, (d, ref) in enumerate(zip(dists, refs)):
             assert_images_eq(d, ref, "plan run %d image %d" % (run, k))
     chosen = plan.autotune(reps=1)
-    assert chosen["ctas_per_sm"] in (2, 3, 4) and 1 <= chosen["grid_percent"] <= 100
+    assert (chosen["ctas_per_sm"], chosen["warps_per_cta"]) in SHAPES and 1 <= chosen["grid_percent"] <= 100
     for d in dists:
         d.fill_(-1.0)
     plan.run()
@@ -389,25 +389,30 @@ def test_plan_graph_runs_match_oracle_and_autotune_keeps_results(ctx):
     plan.close()
 
 
-TUNINGS = [  # (ctas_per_sm, grid_percent, staging, queue_buckets, bucket_width_pct)
-    (3, 100, 1, 8, 50), (4, 50, 1, 8, 50), (2, 25, 1, 8, 50),    # launch shapes, self-staging visits
-    (3, 100, 2, 8, 50), (2, 75, 2, 16, 25),                        # next tile staged ahead
-    (3, 100, 1, 1, 50), (3, 100, 2, 1, 50),                        # FIFO queue
-    (3, 100, 1, 16, 100), (3, 100, 2, 2, 400), (3, 100, 2, 4, 1),  # bucket counts and widths
+SHAPES = {(2, 4), (3, 4), (4, 4), (6, 2), (2, 6), (2, 8)}  # (CTAs per SM, warps per CTA) of the tile kernel
+
+TUNINGS = [  # (ctas_per_sm, grid_percent, staging, queue_buckets, bucket_width_pct, warps_per_cta)
+    (3, 100, 1, 8, 50, 4), (4, 50, 1, 8, 50, 4), (2, 25, 1, 8, 50, 4),    # launch shapes, self-staging visits
+    (6, 100, 1, 8, 25, 2), (2, 100, 1, 8, 25, 6), (2, 60, 1, 1, 50, 8),   # other warps per CTA
+    (3, 100, 2, 8, 50, 4), (2, 75, 2, 16, 25, 4),                         # next tile staged ahead
+    (3, 100, 1, 1, 50, 4), (3, 100, 2, 1, 50, 4),                         # FIFO queue
+    (3, 100, 1, 16, 100, 4), (3, 100, 2, 2, 400, 4), (3, 100, 2, 4, 1, 4),  # bucket counts and widths
 ]
 
 
-@pytest.mark.parametrize("ctas,pct,staging,buckets,width", TUNINGS)
-def test_every_tuning_gives_the_same_map(ctas, pct, staging, buckets, width):
+@pytest.mark.parametrize("ctas,pct,staging,buckets,width,wpc", TUNINGS)
+def test_every_tuning_gives_the_same_map(ctas, pct, staging, buckets, width, wpc):
     """Launch shape, staging and queue policy change the visit order only: every one gives the oracle's map,
     on a single image and on a ragged batch (gray and rgb8, seeds in several tiles)."""
     c = dtb.Context(0)
-    c.set_tuning(ctas_per_sm=ctas, grid_percent=pct, staging=staging, queue_buckets=buckets, bucket_width_pct=width)
+    c.set_tuning(ctas_per_sm=ctas, grid_percent=pct, staging=staging, queue_buckets=buckets, bucket_width_pct=width,
+                 warps_per_cta=wpc)
     assert c.get_tuning() == {"ctas_per_sm": ctas, "grid_percent": pct, "host_chunk_kpx": 16384,
-                              "queue_buckets": buckets, "bucket_width_pct": width, "staging": staging}
+                              "queue_buckets": buckets, "bucket_width_pct": width, "staging": staging,
+                              "warps_per_cta": wpc}
     img, mask, gamma = wl.config0(seed=9)
     d = dtb.geodesic_distance_transform(cuda(img), cuda(mask), gamma, ctx=c)
-    what = "tuning %s" % ((ctas, pct, staging, buckets, width),)
+    what = "tuning %s" % ((ctas, pct, staging, buckets, width, wpc),)
     assert_images_eq(d, orc.ggdt_ns(img, mask, gamma), what)
     batch = wl.config3(seed=31, n=20, smin=48, smax=700)
     dists = dtb.geodesic_distance_transform_batch([cuda(i) for i, _, _ in batch], [cuda(m) for _, m, _ in batch],
@@ -421,7 +426,8 @@ def test_every_tuning_gives_the_same_map(ctas, pct, staging, buckets, width):
 def test_invalid_tunings_are_rejected():
     c = dtb.Context(0)
     for kw in ({"ctas_per_sm": 4, "staging": 2}, {"ctas_per_sm": 5}, {"queue_buckets": 3}, {"queue_buckets": 32},
-               {"bucket_width_pct": 6401}, {"staging": 3}, {"grid_percent": 101}):
+               {"bucket_width_pct": 6401}, {"staging": 3}, {"grid_percent": 101}, {"warps_per_cta": 3},
+               {"ctas_per_sm": 3, "warps_per_cta": 8}, {"ctas_per_sm": 6, "warps_per_cta": 2, "staging": 2}):
         with pytest.raises(dtb.DtbError):
             c.set_tuning(**kw)
     c.close()
