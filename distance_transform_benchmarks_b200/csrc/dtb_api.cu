@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(128) ggdt_scan(const ImgDesc* __restrict__ des
   }
 }
 
-// Persistent tile worker.  Every warp loops: pop a tile, visit it, until the queue drains.
+// Persistent tile worker.  Every warp loops: take the tile its last visit kept (QueueSched::keep_out) or pop
+// one, visit it, until the queue drains.
 template <int MODE, int WPC, int MINB>
 __global__ void __launch_bounds__(WPC * 32, MINB)
     ggdt_persistent(const ImgDesc* __restrict__ descs, const CUtensorMap* __restrict__ tmaps, uint32_t* states, Queue q) {
@@ -77,12 +78,20 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
   WarpSmem& sm = warp_slot(smem_raw);
   warp_slot_init(sm);
   uint32_t parity = 0;
-  const QueueSched sch{q, states};
   const int lane = threadIdx.x & 31;
+  if (lane == 0) sm.keep = POP_NONE;
+  __syncwarp();
+  const QueueSched sch{q, states, &sm.keep};
   WarpStats ws;
   for (;;) {
-    const uint32_t t = queue_pop(q);
-    if (t == POP_NONE) break;
+    uint32_t t = sm.keep;
+    __syncwarp();
+    if (t == POP_NONE) {
+      t = queue_pop(q);
+      if (t == POP_NONE) break;
+    } else if (lane == 0) {
+      sm.keep = POP_NONE;
+    }
     uint32_t old = 0;
     if (lane == 0) {
       old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);

@@ -119,6 +119,7 @@ struct alignas(128) WarpSmem {
   float Wv[(TILE + 1) * W_STRIDE];           // ns-mode: Wv[y * 36 + x] = weight of edge (y-1, y) on column x, y = 0..32;
                                              // its first 1 KB receives the seed-mask TMA box before the weights
   uint64_t bar;                              // TMA mbarrier
+  uint32_t keep;                             // tile this warp keeps for its next visit (POP_NONE: none)
 };
 __device__ __forceinline__ uint8_t* mask_box(WarpSmem& sm) { return reinterpret_cast<uint8_t*>(sm.Wv); }
 
@@ -241,6 +242,18 @@ __device__ __forceinline__ uint32_t bucket_of(const Queue& q, float key, float i
   if (q.nb_mask == 0) return 0;
   const uint32_t base = ld_volatile(&q.hdr->base.v);
   const float r = key * inv_width;  // absolute bucket; NaN / huge values land in the last bucket
+  uint32_t rel = q.nb_mask;
+  if (r < 4.0e9f) {
+    const uint32_t kb = (uint32_t)r;
+    rel = kb <= base ? 0u : min(kb - base, q.nb_mask);
+  }
+  return (base + rel) & q.nb_mask;
+}
+
+// Bucket of an activation value relative to a base the caller read (bucket_of with the base given).
+__device__ __forceinline__ uint32_t bucket_at(const Queue& q, float key, float inv_width, uint32_t base) {
+  if (q.nb_mask == 0) return 0;
+  const float r = key * inv_width;
   uint32_t rel = q.nb_mask;
   if (r < 4.0e9f) {
     const uint32_t kb = (uint32_t)r;

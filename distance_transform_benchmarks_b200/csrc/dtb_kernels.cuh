@@ -31,6 +31,11 @@ struct WarpStats {
 struct QueueSched {
   Queue q;
   uint32_t* states;
+  // Optional: the warp's word for a tile it keeps.  Of the tiles a visit queues, one in the lowest bucket
+  // (the one the workers take from: its activation value is among the smallest queued) is not pushed; the warp
+  // visits it next, which saves the ring's push and pop (two to five L2 round trips) and reuses the halo just
+  // written.  It stays counted in `pending` like a queued tile.  nullptr: every tile goes through the ring.
+  uint32_t* keep_out = nullptr;
   // Warp-level end of a visit.  Lanes with `want` ask for a re-run of neighbour `item`, bringing activation
   // value `key` (distance units; bucket width 1 / inv_width): idle -> queued; running -> running with a re-run
   // requested; queued -> unchanged.  Lane 31 clears RUNNING of the own tile (and sets / clears the xor_bits);
@@ -82,10 +87,19 @@ struct QueueSched {
       fence_acq_rel();
     }
     __syncwarp();
-    if (push) {
-      const uint32_t b = bucket_of(q, pkey, inv_width);
-      slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
+    uint32_t base = 0;
+    if (q.nb_mask) base = ld_volatile(&q.hdr->base.v);
+    const uint32_t b = push ? bucket_at(q, pkey, inv_width, base) : 0u;
+    int kept = -1;
+    if (keep_out) {
+      const bool elig = push && b == (base & q.nb_mask);
+      const uint32_t kmin = __reduce_min_sync(~0u, elig ? __float_as_uint(pkey) : 0xFFFFFFFFu);
+      const uint32_t cand = __ballot_sync(~0u, elig && __float_as_uint(pkey) == kmin);
+      if (cand) kept = __ffs(cand) - 1;
+      if (lane == kept) *keep_out = item;
     }
+    if (push && lane != kept) slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
+    __syncwarp();
     if (__shfl_sync(~0u, last, 0)) signal_done_warp(q);
   }
 };
