@@ -8,6 +8,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -226,6 +227,20 @@ __global__ void __launch_bounds__(128) ggdt_finalize(const ImgDesc* __restrict__
 // Host side
 // ======================================================================================================
 namespace dtb {
+
+static nvtxDomainHandle_t trace_domain() {
+  static nvtxDomainHandle_t d = nvtxDomainCreateA("dtb");
+  return d;
+}
+TraceRange::TraceRange(const char* name) {
+  nvtxEventAttributes_t a{};
+  a.version = NVTX_VERSION;
+  a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+  a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+  a.message.ascii = name;
+  nvtxDomainRangePushEx(trace_domain(), &a);
+}
+TraceRange::~TraceRange() { nvtxDomainRangePop(trace_domain()); }
 
 dtb_status fail(dtb_context ctx, dtb_status s, const char* fmt, ...) {
   char buf[512];
@@ -577,6 +592,7 @@ static bool dist_ok(const dtb_image* im) {
 
 dtb_status run_jobs(dtb_context ctx, const std::vector<Job>& jobs_in, const dtb_image* const* imgs,
                     const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags, cudaStream_t stream) {
+  const TraceRange trace("dtb call");
   const int n = (int)jobs_in.size();
   std::vector<Job> jobs = jobs_in;
 

@@ -131,6 +131,7 @@ void place_plane(int a, int b, const std::vector<HostPlane>& hp, Take&& take, st
 dtb_status run_host_pipeline(dtb_context ctx, std::vector<Job> jobs, const dtb_image* const* imgs,
                              const dtb_image* const* masks, const dtb_image* const* dists, uint32_t flags,
                              cudaStream_t stream) {
+  const TraceRange trace("dtb host pipeline");
   const int n = (int)jobs.size();
   if (!ctx->s_in) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_in, cudaStreamNonBlocking));
   if (!ctx->s_out) DTB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->s_out, cudaStreamNonBlocking));

@@ -172,6 +172,15 @@ struct dtb_context_s {
 
 namespace dtb {
 
+// A named range on a profiler's host timeline (NVTX domain "dtb": calls, plan runs, the autotuner, serve waves,
+// live publishes and launches); header-only NVTX, which costs nothing when no profiler is attached.
+struct TraceRange {
+  explicit TraceRange(const char* name);
+  ~TraceRange();
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+
 dtb_status fail(dtb_context ctx, dtb_status s, const char* fmt, ...);
 dtb_status cuda_fail(dtb_context ctx, cudaError_t e, const char* what);
 #define DTB_CUDA(ctx, call)                                    \

@@ -258,6 +258,7 @@ DTB_API dtb_status dtb_plan_create(dtb_context ctx, int32_t n, const dtb_image* 
 
 DTB_API dtb_status dtb_plan_run(dtb_plan p, void* stream) {
   if (!p || !p->exec) return DTB_ERR_INVALID_ARG;
+  const TraceRange trace("dtb plan run");
   DTB_CUDA(p->ctx, cudaGraphLaunch(p->exec, reinterpret_cast<cudaStream_t>(stream)));
   return DTB_OK;
 }
@@ -277,6 +278,7 @@ DTB_API dtb_status dtb_plan_wait(dtb_plan p, void* stream, dtb_stats* stats) {
 
 DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb_tuning* chosen) {
   if (!p || reps < 1) return DTB_ERR_INVALID_ARG;
+  const TraceRange trace("dtb autotune");
   dtb_context ctx = p->ctx;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   cudaEvent_t a, b;

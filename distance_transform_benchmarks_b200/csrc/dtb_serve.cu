@@ -419,6 +419,7 @@ struct InFlight {
 // helpers below record failures in the context's message).  Requests of the wave reference no image of another wave in flight (admit), so the
 // waves' device work only shares the arena's free space and the tile-run stream.
 dtb_status launch_wave(dtb_server s, InFlight& f) {
+  const TraceRange trace("dtb serve wave");
   dtb_context ctx = s->ctx;
   cudaStream_t st = s->s_run;
   WaveSlot& ws = s->slot[f.slot];
@@ -1011,6 +1012,7 @@ std::vector<LiveFlight> live_admit_host(dtb_server s) {
 // Copies one admitted request in and publishes it (s_in, in order: data, descriptor + maps, entry, count).  The
 // caller holds the context's lock.
 dtb_status live_publish(dtb_server s, LiveFlight& f, const Resident& r) {
+  const TraceRange trace("dtb live publish");
   dtb_context ctx = s->ctx;
   LiveEngine* L = s->live;
   cudaStream_t st = s->s_in;
@@ -1109,6 +1111,7 @@ dtb_status live_publish(dtb_server s, LiveFlight& f, const Resident& r) {
 
 // Launches the live kernel (queue header and ring reset first, on the tile-run stream).
 dtb_status live_launch(dtb_server s) {
+  const TraceRange trace("dtb live launch");
   dtb_context ctx = s->ctx;
   LiveEngine* L = s->live;
   cudaStream_t st = s->s_run;
