@@ -84,15 +84,18 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
   __syncwarp();
   const QueueSched sch{q, states, &sm.keep};
   WarpStats ws;
+  uint32_t prev = POP_NONE;  // the tile this warp visited last
   for (;;) {
     uint32_t t = sm.keep;
     __syncwarp();
+    const bool again = t != POP_NONE && t == prev;  // kept its own tile: its weights and distances are in smem
     if (t == POP_NONE) {
       t = queue_pop(q);
       if (t == POP_NONE) break;
     } else if (lane == 0) {
       sm.keep = POP_NONE;
     }
+    prev = t;
     uint32_t old = 0;
     if (lane == 0) {
       old = atomicXor(&states[t], ST_PENDING | ST_RUNNING);
@@ -102,7 +105,8 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     const uint32_t img = old >> ST_IMG_SHIFT;
     if constexpr (MODE == MODE_NS) {
       const ImgDesc dd = descs[img];
-      visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws);
+      // A re-run needs the tile visited (weights and B from that visit) and no new seeds to apply.
+      visit_tile<MODE>(dd, tmaps, img, t, old, sm, parity, sch, ws, again && (old & ST_VISITED) && !(old & ST_SEED));
     } else {
       // ref-mode reads the descriptor fields where it uses them (read-only, cached) instead of holding a copy
       // in registers through the visit.

@@ -92,10 +92,17 @@ struct QueueSched {
     const uint32_t b = push ? bucket_at(q, pkey, inv_width, base) : 0u;
     int kept = -1;
     if (keep_out) {
+      // The own tile first (lane 31 re-queues it when its halo dropped during the visit): its re-run reuses the
+      // weights and distances in this warp's shared memory.  Else the smallest activation value.
       const bool elig = push && b == (base & q.nb_mask);
-      const uint32_t kmin = __reduce_min_sync(~0u, elig ? __float_as_uint(pkey) : 0xFFFFFFFFu);
-      const uint32_t cand = __ballot_sync(~0u, elig && __float_as_uint(pkey) == kmin);
-      if (cand) kept = __ffs(cand) - 1;
+      const uint32_t em = __ballot_sync(~0u, elig);
+      if (em >> 31) {
+        kept = 31;
+      } else {
+        const uint32_t kmin = __reduce_min_sync(~0u, elig ? __float_as_uint(pkey) : 0xFFFFFFFFu);
+        const uint32_t cand = __ballot_sync(~0u, elig && __float_as_uint(pkey) == kmin);
+        if (cand) kept = __ffs(cand) - 1;
+      }
       if (lane == kept) *keep_out = item;
     }
     if (push && lane != kept) slot_write(q, b, atomicAdd(&q.hdr->tails[b].v, 1u), item);
@@ -290,11 +297,16 @@ __device__ __forceinline__ void store_row(float* row, const float (&d)[TILE]) {
 // B.  Element k of lane l is at [k * 36 + l] of the row-major arrays in the column layout (scalar loads), at
 // [l * 36 + k] in the row layout (16-byte vectors).
 // Returns the number of phases and activations through *nph / *nact.
+//
+// rerun: the warp visits again the tile it has just visited (its halo dropped while it ran, and the visit kept
+// it).  The warp's shared memory still holds that tile's edge weights (Wh / Wv) and its final distances (the
+// tile buffer B, equal to the tile in global memory: no other warp can have visited it in between), so the
+// re-run reloads only the neighbour states and halos: no bulk copy, no weights, no tile loads.
 // ------------------------------------------------------------------------------------------------------
 template <bool PRESTAGED, class Sched>
 __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
                                          uint32_t tile, uint32_t old_state, const VisitBufs& vb, const Sched& sch,
-                                         uint32_t* nph_out, uint32_t* nact_out) {
+                                         uint32_t* nph_out, uint32_t* nact_out, bool rerun = false) {
   const int lane = threadIdx.x & 31;
   const float INF = f_inf();
   const uint32_t local = tile - dd.tile_base;
@@ -308,8 +320,12 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   *nph_out = 0;
   *nact_out = 0;
 
-  if (!PRESTAGED) stage_tile(vb, tm_img, tm_mask, rgb, seed, x0, y0);
-  else if (seed) stage_box(vb.Wv, vb.mbar, tm_mask, TILE * TILE, x0, y0);
+  if (rerun) {
+  } else if (!PRESTAGED) {
+    stage_tile(vb, tm_img, tm_mask, rgb, seed, x0, y0);
+  } else if (seed) {
+    stage_box(vb.Wv, vb.mbar, tm_mask, TILE * TILE, x0, y0);
+  }
 
   // Neighbour states: lane 0 left, 1 right, 2 top, 3 bottom.
   const uint32_t nexist = (tx > 0 ? 1u : 0u) | (tx + 1 < dd.tiles_x ? 2u : 0u) | (ty > 0 ? 4u : 0u) |
@@ -338,13 +354,17 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
 
   // Tile distances in column layout.
   float d[TILE];
-  if (!first) {
+  if (rerun) {
+    const float* pb = reinterpret_cast<const float*>(vb.box) + lane;  // B[y * 36 + x]
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) d[y] = pb[y * W_STRIDE];
+  } else if (!first) {
     const uint8_t* lb = dist_base(dd, y0, x0 + lane, 0u);
 #pragma unroll
     for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist_at(lb, dd.dist_pitch, y) : INF;
   }
 
-  if (!tma_wait(vb.bar, *vb.pbits, vb.pmask, sch.q, tile)) return;
+  if (!rerun && !tma_wait(vb.bar, *vb.pbits, vb.pmask, sch.q, tile)) return;
   if (PRESTAGED && seed && !tma_wait(vb.mbar, *vb.pbits, vb.mmask, sch.q, tile)) return;
   const uint8_t* mbox = reinterpret_cast<const uint8_t*>(vb.Wv);
 
@@ -364,8 +384,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
   __syncwarp();
 
   // Edge weights into Wh / Wv (computed in column layout, lane = x).  Edges touching a pixel outside the image
-  // are INF.
-  {
+  // are INF.  A re-run has them from its previous visit.
+  if (!rerun) {
     const float g2 = dd.g2;
     const uint8_t* box = vb.box;
     if (!rgb) {
@@ -886,12 +906,12 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
 template <int MODE, class Sched>
 __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap* tmaps, uint32_t img, uint32_t tile,
                                            uint32_t old_state, WarpSmem& sm, uint32_t& parity, const Sched& sch,
-                                           WarpStats& ws) {
+                                           WarpStats& ws, bool rerun = false) {
   const CUtensorMap* tm_img = tmaps + 2 * img;
   const CUtensorMap* tm_mask = tmaps + 2 * img + 1;
   uint32_t nph, nact;
   if (MODE == MODE_NS)
-    visit_ns<false>(dd, tm_img, tm_mask, tile, old_state, visit_bufs(sm, parity), sch, &nph, &nact);
+    visit_ns<false>(dd, tm_img, tm_mask, tile, old_state, visit_bufs(sm, parity), sch, &nph, &nact, rerun);
   else if (MODE == MODE_REF)
     visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
   else
