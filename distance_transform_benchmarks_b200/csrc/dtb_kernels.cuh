@@ -96,7 +96,7 @@ struct QueueSched {
       // weights and distances in this warp's shared memory.  Else the smallest activation value.
       const bool elig = push && b == (base & q.nb_mask);
       const uint32_t em = __ballot_sync(~0u, elig);
-      if (em >> 31) {
+      if (__ballot_sync(~0u, push) >> 31) {  // the own tile, whatever its bucket: its re-run is cheap
         kept = 31;
       } else {
         const uint32_t kmin = __reduce_min_sync(~0u, elig ? __float_as_uint(pkey) : 0xFFFFFFFFu);

@@ -165,6 +165,10 @@ struct LiveSched {
   Queue q;
   uint32_t* states;
   const LiveArgs* a;
+  // The warp's word for its own tile when its halo dropped during the visit: the warp re-runs it next from the
+  // weights and distances in its shared memory (neighbour tiles always go through the ring, so that warps come
+  // back to the queue, where new requests are claimed).
+  uint32_t* keep_out;
   __device__ __forceinline__ void complete(uint32_t tile, uint32_t xor_bits, bool want, uint32_t want_item,
                                            float = 0.0f, float = 0.0f) const {
     const int lane = threadIdx.x & 31;
@@ -201,7 +205,10 @@ struct LiveSched {
       __threadfence();
     }
     __syncwarp();
-    if (push) live_push(q, item);
+    const bool keep_own = (__ballot_sync(~0u, push) >> 31) != 0u;
+    if (lane == 31 && keep_own) *keep_out = item;
+    if (push && !(lane == 31 && keep_own)) live_push(q, item);
+    __syncwarp();
     if (__shfl_sync(~0u, last, 0)) live_finish(*a, slot);
   }
 };
@@ -552,11 +559,20 @@ __global__ void __launch_bounds__(WPC * 32, MINB) ggdt_live(LiveArgs a) {
   uint32_t t_start = 0;
   if (lane == 0) t_start = now_us();
   t_start = __shfl_sync(~0u, t_start, 0);
-  const LiveSched sch{a.q, a.states, &a};
+  if (lane == 0) sm.keep = POP_NONE;
+  __syncwarp();
+  const LiveSched sch{a.q, a.states, &a, &sm.keep};
   WarpStats ws;
   for (;;) {
-    const uint32_t it = live_pop(a, t_start);
-    if (it == POP_NONE) break;
+    uint32_t it = sm.keep;  // the own tile the last visit kept (a re-run), else the queue and admissions
+    __syncwarp();
+    const bool again = it != POP_NONE;
+    if (!again) {
+      it = live_pop(a, t_start);
+      if (it == POP_NONE) break;
+    } else if (lane == 0) {
+      sm.keep = POP_NONE;
+    }
     if (it & LIVE_JOB) {
       live_job(a, it);
       continue;
@@ -570,7 +586,8 @@ __global__ void __launch_bounds__(WPC * 32, MINB) ggdt_live(LiveArgs a) {
     // drew into, by generic stores; the visit reads them by bulk copy (async proxy).
     if ((old & ST_SEED) || !(old & ST_VISITED)) asm volatile("fence.proxy.async.global;" ::: "memory");
     uint32_t nph, nact;
-    visit_ns<false>(dd, a.tmaps + 2 * slot, a.tmaps + 2 * slot + 1, it, old, visit_bufs(sm, parity), sch, &nph, &nact);
+    visit_ns<false>(dd, a.tmaps + 2 * slot, a.tmaps + 2 * slot + 1, it, old, visit_bufs(sm, parity), sch, &nph, &nact,
+                    again && (old & ST_VISITED) && !(old & ST_SEED));
     count_visit(ws, a.q, nph, nact);
   }
   flush_stats(ws, a.q);
