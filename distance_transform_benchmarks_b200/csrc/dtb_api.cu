@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(WPC * 32, MINB)
     } else {
       // ref-mode reads the descriptor fields where it uses them (read-only, cached) instead of holding a copy
       // in registers through the visit.
-      visit_tile<MODE>(descs[img], tmaps, img, t, old, sm, parity, sch, ws);
+      visit_tile<MODE>(descs[img], tmaps, img, t, old, sm, parity, sch, ws,
+                       again && (old & ST_VISITED) && !(old & ST_SEED));
     }
   }
   flush_stats(ws, q);

@@ -616,7 +616,10 @@ __device__ __forceinline__ float ref_min3(float cur, float da, float db, float d
 template <bool FMA, class Sched>
 __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* tm_img, const CUtensorMap* tm_mask,
                                           uint32_t tile, uint32_t old_state, WarpSmem& sm, uint32_t& parity,
-                                          const Sched& sch, uint32_t* nph_out, uint32_t* nact_out) {
+                                          const Sched& sch, uint32_t* nph_out, uint32_t* nact_out,
+                                          bool rerun = false) {
+  // rerun: as in visit_ns -- the padded image lines (pimg / pimgT) and the tile values (T) of this tile's previous
+  // visit are still in the warp's shared memory; only the neighbour states and halos are read again.
   *nph_out = 0;
   *nact_out = 0;
   const int lane = threadIdx.x & 31;
@@ -631,7 +634,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   const float sq2 = 1.41421354f;  // sqrtf(2.f), reference generalised_distance_transform.cu:111
 
   const VisitBufs vb = visit_bufs(sm, parity);
-  stage_tile(vb, tm_img, tm_mask, false, seed, x0, y0);
+  if (!rerun) stage_tile(vb, tm_img, tm_mask, false, seed, x0, y0);
 
   // Neighbour k = lane (0..7): (dx, dy) = L, R, T, B, TL, TR, BL, BR.
   // Offsets of neighbour k = lane, the tables {-1,1,0,0,-1,1,-1,1} and {0,0,-1,1,-1,-1,1,1} as bit masks (an
@@ -674,21 +677,26 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
     hb[TILE + 1] = br; hr[TILE + 1] = br;
   }
 
+  // Tile values live in T (column-layout transposes) = sm.img region after staging is consumed.
+  float* T = reinterpret_cast<float*>(sm.img);  // 32 x 33 floats = 4224 bytes <= 4352
   float d[TILE];
-  if (!first) {
+  if (rerun) {
+#pragma unroll
+    for (int y = 0; y < TILE; ++y) d[y] = T[y * S_STRIDE + lane];
+  } else if (!first) {
     const uint8_t* lb = dist_base(dd, y0, x0 + lane, 0u);
 #pragma unroll
     for (int y = 0; y < TILE; ++y) d[y] = (lane < vw && y < vh) ? ld_dist_at(lb, dd.dist_pitch, y) : INF;
   }
 
-  if (!tma_wait(&sm.bar, parity, 1u, sch.q, tile)) return;
+  if (!rerun && !tma_wait(&sm.bar, parity, 1u, sch.q, tile)) return;
 
   // Padded copies of the image box, one line per tile row and one per tile column (position -1..32 at byte
   // pos + 1): pimg line r = box row r (tile row r - 1), pimgT line c = tile column c - 1.  In either layout
-  // lane l needs lines l, l + 1, l + 2 (its own line and the two beside it) of one of them.
+  // lane l needs lines l, l + 1, l + 2 (its own line and the two beside it) of one of them.  A re-run has them.
   uint8_t* pimg = reinterpret_cast<uint8_t*>(sm.Wh + 96);    // 34 * 36 = 1224 bytes after the halo rows
   uint8_t* pimgT = reinterpret_cast<uint8_t*>(sm.Wh + 416);  // 1224 bytes after pimg
-  for (int i = lane; i < IMG_BOX_ROWS * PIMG_STRIDE; i += 32) {
+  for (int i = lane; !rerun && i < IMG_BOX_ROWS * PIMG_STRIDE; i += 32) {
     const int r = i / PIMG_STRIDE, c = i % PIMG_STRIDE;
     const uint8_t px = (c < TILE + 2) ? sm.img[r * IMG_BOX_GRAY + 15 + c] : 0;
     pimg[i] = px;
@@ -708,9 +716,7 @@ __device__ __forceinline__ void visit_ref(const ImgDesc& dd, const CUtensorMap* 
   }
   __syncwarp();
 
-  // Tile values live in T (column-layout transposes) = sm.img region after staging is consumed:
-  // the image is needed through pimg only from here on.
-  float* T = reinterpret_cast<float*>(sm.img);  // 32 x 33 floats = 4224 bytes <= 4352
+  // From here on the image is needed through pimg only; T holds the tile.
   // Initial border values for the change test, kept in shared memory through the phases (registers are the
   // scarce resource there): top, bottom, left, right at border0[32 * side + lane].
   float* border0 = sm.Wv + 352;  // after the halo columns
@@ -913,9 +919,9 @@ __device__ __forceinline__ void visit_tile(const ImgDesc& dd, const CUtensorMap*
   if (MODE == MODE_NS)
     visit_ns<false>(dd, tm_img, tm_mask, tile, old_state, visit_bufs(sm, parity), sch, &nph, &nact, rerun);
   else if (MODE == MODE_REF)
-    visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
+    visit_ref<true>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact, rerun);
   else
-    visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact);
+    visit_ref<false>(dd, tm_img, tm_mask, tile, old_state, sm, parity, sch, &nph, &nact, rerun);
   count_visit(ws, sch.q, nph, nact);
 }
 
