@@ -205,7 +205,7 @@ struct LiveSched {
       __threadfence();
     }
     __syncwarp();
-    const bool keep_own = (__ballot_sync(~0u, push) >> 31) != 0u;
+    const bool keep_own = (m >> 31) != 0u;  // lane 31 re-queues the own tile (activations are lanes 0-3)
     if (lane == 31 && keep_own) *keep_out = item;
     if (push && !(lane == 31 && keep_own)) live_push(q, item);
     __syncwarp();
