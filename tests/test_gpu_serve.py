@@ -305,3 +305,30 @@ def test_live_kernel_ends_when_idle_relaunches_and_allocates_nothing():
     assert st["failed"] == 0 and st["waves"] >= 7, st  # a launch per request after each idle end
     assert st["tile_visits"] > 0 and st["kernel_ms"] > 0
     srv.close()
+
+
+@BOTH
+def test_odd_shapes_and_their_edits_match_the_oracle(live):
+    """Edge shapes through both engines: one-pixel and one-row / one-column images, sides that are not multiples
+    of the 32-pixel tile or of 16 bytes, and a 1023 x 8 rgb8 image whose staged rows do not fit its distance plane
+    (live engine: the copy goes straight into place instead); each new image and one edit of it equal the
+    oracle's map."""
+    rng = np.random.default_rng(11)
+    shapes = [(1, 1, 1), (33, 1, 1), (1, 57, 1), (1023, 8, 3), (257, 3, 3), (31, 95, 1), (65, 33, 3)]
+    srv = dtb.Server(64 << 20, live=live)
+    for k, (w, h, c) in enumerate(shapes):
+        img = (wl.blobs_gray(100 + k, w, h) if c == 1 else wl.voronoi_rgb(100 + k, w, h))
+        mask = np.zeros((h, w), np.uint8)
+        mask[int(rng.integers(0, h)), int(rng.integers(0, w))] = 1
+        g = 0.1
+        out = torch.empty((h, w), dtype=torch.float32)
+        rid = srv.submit_image(k, torch.from_numpy(img), torch.from_numpy(mask), g, out)
+        assert _drain(srv, 1)[rid]["status"] == 0
+        assert_images_eq(out, orc.ggdt_ns(img, mask, g), "image %dx%dx%d" % (w, h, c))
+        disks = [(int(rng.integers(0, w)), int(rng.integers(0, h)), 1)]
+        out2 = torch.empty((h, w), dtype=torch.float32)
+        rid = srv.submit_edit(k, disks, out2)
+        assert _drain(srv, 1)[rid]["status"] == 0
+        assert_images_eq(out2, orc.ggdt_ns(img, _mask_with(mask, disks), g), "edit of %dx%dx%d" % (w, h, c))
+    assert srv.stats()["failed"] == 0
+    srv.close()
