@@ -107,6 +107,7 @@ class DtbError(RuntimeError):
 
 _lib = None
 _host = None
+ABI_VERSION = 3  # the struct layouts mirrored here (include/dtb.h DTB_ABI_VERSION)
 
 
 def lib():
@@ -119,6 +120,9 @@ def lib():
         P, I32, U32, F = ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32, ctypes.c_float
         IMG = ctypes.POINTER(DtbImage)
         L.dtb_abi_version.restype = I32
+        if L.dtb_abi_version() != ABI_VERSION:
+            raise RuntimeError("libdtb.so has ABI version %d, this package mirrors %d: rebuild it with "
+                               "__graft_entry__.build()" % (L.dtb_abi_version(), ABI_VERSION))
         L.dtb_status_string.restype = ctypes.c_char_p
         L.dtb_status_string.argtypes = [I32]
         L.dtb_context_create.restype = I32

@@ -21,7 +21,7 @@ extern "C" {
 #endif
 
 #define DTB_API __attribute__((visibility("default")))
-#define DTB_ABI_VERSION 2
+#define DTB_ABI_VERSION 3  /* 3: dtb_tuning.warps_per_cta, dtb_serve_config.live*, dtb_serve_stats.live_ended_* */
 
 typedef enum dtb_status {
   DTB_OK = 0,

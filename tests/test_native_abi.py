@@ -28,7 +28,7 @@ def test_libdtb_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = _native.lib()
-    assert lib.dtb_abi_version() == 2
+    assert lib.dtb_abi_version() == _native.ABI_VERSION == 3
     assert lib.dtb_status_string(0) == b"ok"
     assert lib.dtb_status_string(4) == b"device wait timed out"
     assert lib.dtb_status_string(99) == b"unknown status"
