@@ -1,5 +1,5 @@
 // dtb_plan.cu -- batch plans: a ragged ns-mode batch prepared once, captured in a CUDA graph, run many times;
-// the autotuner that picks the tile-kernel variant (CTAs per SM, staging), grid share and tile-queue policy
+// the autotuner that picks the tile-kernel variant (CTAs per SM x warps per CTA, staging), grid share and tile-queue policy
 // (FIFO or distance-ordered buckets, their count and width) for a batch; and its JSON cache, keyed by GPU
 // name and workload size class, which later processes reuse.
 #include <cuda_runtime.h>
@@ -312,7 +312,7 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
     }
   };
   // Coordinate search: (1) kernel variant (CTAs per SM x warps per CTA x staging) x grid share under the current
-  // queue policy; (2) queue policy (FIFO; 8 or 16 buckets of 1/4, 1/2 or 1 tile-width) under the best launch;
+  // queue policy; (2) queue policy (FIFO; 8 or 16 buckets of 1/10, 1/4, 1/2 or 1 tile-width) under the best launch;
   // (3) the variants again under the best policy.
   static const int kPercent[3] = {100, 75, 50};
   const LaunchTuning start = p->tuning;
@@ -329,7 +329,7 @@ DTB_API dtb_status dtb_plan_autotune(dtb_plan p, void* stream, int32_t reps, dtb
     t.buckets = 1;
     trial(t);
     static const int kBuckets[2] = {8, 16};
-    static const float kWidth[3] = {0.25f, 0.5f, 1.0f};
+    static const float kWidth[4] = {0.1f, 0.25f, 0.5f, 1.0f};
     for (int nb : kBuckets)
       for (float w : kWidth) {
         t = launch;
