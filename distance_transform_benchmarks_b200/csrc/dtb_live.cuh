@@ -298,7 +298,7 @@ __device__ bool live_admit(const LiveArgs& a, uint32_t t_start) {
     __threadfence();
     __syncwarp();
     // Queue the tiles the disks touch (as serve_seed_tiles); the image has no other request in flight, so every
-    // tile is idle and VISITED.
+    // tile is idle: VISITED with its map, or never reached, holding v, where its first visit starts from v too.
     for (uint32_t k = 0; k < nd; ++k) {
       const int4 dk = __ldcg(reinterpret_cast<const int4*>(a.disks) + (di + k));
       const int cx = dk.x, cy = dk.y, r = dk.z;
